@@ -1,0 +1,56 @@
+/*
+ * qas_oracle.h -- plain-C restatement of qasMHD's per-step update.
+ *
+ * TEST INFRASTRUCTURE.  This library is the CPU checker used by tests/,
+ * __graft_entry__.smoke() and the CPU-baseline leg of bench.py.  The product
+ * (libqas, include/qas.h) never links or calls it.
+ *
+ * State layout: one contiguous block of 8*nd doubles, field m at u + m*nd,
+ * fields (ro,mx,my,mz,bx,by,bz,en), cell ss = nx*(ny*k+j)+i with 4 ghost
+ * cells per side (2D/SERIAL/OTvortex/mhd2d_class.cpp:116-164).
+ */
+#ifndef QAS_ORACLE_H
+#define QAS_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int dim;             /* 1, 2 or 3 */
+  int nxm, nym, nzm;   /* interior cells per axis (1 for unused axes) */
+  int rmn;             /* 0 Roe, 1 HLLD, 2 LHLLD, 3 MLAU (common/mhd_class.hpp:102-105) */
+  int odr;             /* spatial order 1..4 */
+  int rk;              /* SSP-RK order 1..3 */
+  int ctw;             /* CUCT upwind weighting on/off */
+  double gam, dx, dy, dz;
+  int dnx[8], dny[8], dnz[8];   /* boundary flags per field */
+} qo_grid;
+
+/* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,
+ * mhd3d_class.cpp:3-13). */
+void qo_bound(const qo_grid *g, double *u);
+
+/* One SSP-RK step of the ideal equations, i.e. MHD{1,2,3}D::ideal(dt), including the
+ * per-stage ghost fill.  Returns 0 on success, -1 on allocation failure. */
+int qo_step(const qo_grid *g, double *u, double dt);
+
+/* max(1, max over interior of |v| + c_f), the reduction inside setdt()
+ * (mhd1d_class.cpp:11-30, mhd2d_class.cpp:11-33, mhd3d_class.cpp:15-46).  `unused`
+ * is ignored (kept for ABI stability of the test binding). */
+double qo_cfl_dt(const qo_grid *g, const double *u, double unused);
+
+/* One visco-resistive stage loop, DMHD2D::dsptv(dt) (2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151)
+ * with uniform nu0, eta0.  2D only. */
+int qo_dsptv(const qo_grid *g, double *u, double dt, double nu0, double eta0);
+
+/* setdc() + sub-cycled dsptv (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26) with uniform nu0, eta0. */
+int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0);
+
+/* Point-function known answers; same function ids and layouts as oracle/ref_harness/ref_kat.cpp. */
+int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,100 @@
+/*
+ * Oracle harness for the reference's 1D stepping code
+ * (1D/SERIAL/shock/mhd1d_solve.cpp:3-124, mhd1d_class.cpp:3-53).
+ * Loop semantics follow MHD1D::exec_ (1D/SERIAL/shock/mhd1d_class.cpp:32-53):
+ * the 1D driver calls exec_(0) (1D/SERIAL/shock/main.cpp), i.e. a constant dt
+ * from the first setdt(1) and nmax = nrec*nout steps.  Test infrastructure only.
+ */
+#include <omp.h>
+#include "mhd1d_class.hpp"
+#include "qas_ref_io.h"
+
+int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
+double qh_dtrec = 1.0, qh_cfl = 0.4;
+
+class RefHarness1D : public MHD1D {
+ public:
+  void setup(const RefCaseHeader &h, const double *data)
+  {
+    setgam(h.gam);
+    xmin = h.xmin; xmax = h.xmax;
+    dx = (xmax - xmin) / XMESH;
+    dt = cfl * dx;
+    for (int i = 0; i < nx; i++) x[i] = (i - xoff + 0.5) * dx + xmin;
+    for (int m = 0; m < nm; m++) dnxs[m] = h.dnx[m];
+    for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nx, sizeof(double) * nx);
+  }
+  void one_step(int flg, std::vector<double> *dts)
+  {
+    tim += dt;
+    dts->push_back(dt);
+    bound(val, nm, dnxs);
+    ideal(dt);
+    setdt(flg * (n % 2 == 0));
+  }
+  int run(const RefCaseHeader &h, std::vector<double> *dts, double *elapsed)
+  {
+    int steps = 0;
+    double t0 = omp_get_wtime();
+    if (h.mode == REF_MODE_STEP) {
+      dt = h.dt;
+      dts->push_back(dt);
+      bound(val, nm, dnxs);
+      ideal(dt);
+      steps = 1;
+    } else if (h.mode == REF_MODE_RUN) {
+      setdt(1);
+      for (int s = 0; s < h.nsteps; s++) {
+        n++;
+        one_step(h.flg, dts);
+        steps++;
+      }
+    } else if (h.mode == REF_MODE_EXEC) {
+      setdt(1);
+      int flg = h.flg;
+      while ((flg) ? (n++ < nmax && tim < tmax) : (n++ < nmax)) {
+        one_step(flg, dts);
+        steps++;
+      }
+    } else {
+      ref_die("unknown mode");
+    }
+    *elapsed = omp_get_wtime() - t0;
+    return steps;
+  }
+  double time_now() const { return tim; }
+  double dt_now() const { return dt; }
+  double *const *state() const { return val; }
+};
+
+int main(int argc, char **argv)
+{
+  if (argc != 3) ref_die("usage: ref1d <case.bin> <result.bin>");
+  RefCaseHeader h;
+  std::vector<double> data;
+  ref_read_case(argv[1], &h, &data);
+  if (h.dim != 1) ref_die("ref1d needs dim=1");
+  qh_xmesh = h.nxm; qh_ymesh = 1; qh_zmesh = 1;
+  qh_rmn = h.rmn; qh_odr = h.odr; qh_rk = h.rk;
+  qh_cfl = h.cfl; qh_dtrec = h.dtrec; qh_nout = h.nout;
+  if (h.nthreads > 0) omp_set_num_threads(h.nthreads);
+
+  RefHarness1D *sim = new RefHarness1D();
+  sim->setup(h, data.data());
+  std::vector<double> dts;
+  double elapsed = 0.0;
+  int steps = sim->run(h, &dts, &elapsed);
+
+  RefResultHeader r;
+  memset(&r, 0, sizeof(r));
+  r.magic = QAS_REF_MAGIC_OUT;
+  r.nsteps_done = steps;
+  r.n_dt = (int)dts.size();
+  r.nd = h.nxm + 8;
+  r.tim = sim->time_now();
+  r.dt = sim->dt_now();
+  r.elapsed_s = elapsed;
+  ref_write_result(argv[2], r, dts, sim->state(), r.nd);
+  delete sim;
+  return 0;
+}

@@ -1,0 +1,107 @@
+/*
+ * Oracle harness for the reference's 3D stepping code, run on one rank
+ * (3D/MPI/KHI/mhd3d_solve.cpp:3-729, mhd3d_class.cpp:3-76, mpi/common_mpi.c)
+ * against the single-rank MPI stand-in in oracle/mpi_stub/mpi.h.
+ * Loop semantics follow MHD3D::exec_ (3D/MPI/KHI/mhd3d_class.cpp:48-76)
+ * without its backup/output side effects.  Test infrastructure only.
+ */
+#include <omp.h>
+#include "mhd3d_class.hpp"
+#include "qas_ref_io.h"
+
+int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
+double qh_dtrec = 1.0, qh_cfl = 0.4;
+
+class RefHarness3D : public MHD3D {
+ public:
+  RefHarness3D(int *argc, char ***argv) : MHD3D(argc, argv, 1) {}
+  void setup(const RefCaseHeader &h, const double *data)
+  {
+    setgam(h.gam);
+    xmin = h.xmin; xmax = h.xmax; ymin = h.ymin; ymax = h.ymax; zmin = h.zmin; zmax = h.zmax;
+    dx = (xmax - xmin) / XMESH;
+    dy = (ymax - ymin) / YMESH;
+    dz = (zmax - zmin) / ZMESH;
+    dr = min(min(dx, dy), dz);
+    dt = cfl * dr;
+    for (int i = 0; i < nx; i++) x[i] = (i - xoff + 0.5) * dx + xmin;
+    for (int j = 0; j < ny; j++) y[j] = (j - yoff + 0.5) * dy + ymin;
+    for (int k = 0; k < nz; k++) z[k] = (k - zoff + 0.5) * dz + zmin;
+    for (int m = 0; m < nm; m++) { dnxs[m] = h.dnx[m]; dnys[m] = h.dny[m]; dnzs[m] = h.dnz[m]; }
+    for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nd, sizeof(double) * nd);
+  }
+  void one_step(int flg, std::vector<double> *dts)
+  {
+    tim += dt;
+    dts->push_back(dt);
+    bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
+    ideal(dt);
+    setdt(flg * (n % 2 == 0));
+  }
+  int run(const RefCaseHeader &h, std::vector<double> *dts, double *elapsed)
+  {
+    int steps = 0;
+    double t0 = omp_get_wtime();
+    if (h.mode == REF_MODE_STEP) {
+      dt = h.dt;
+      dts->push_back(dt);
+      bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
+      ideal(dt);
+      steps = 1;
+    } else if (h.mode == REF_MODE_RUN) {
+      setdt(1);
+      for (int s = 0; s < h.nsteps; s++) {
+        n++;
+        one_step(h.flg, dts);
+        steps++;
+      }
+    } else if (h.mode == REF_MODE_EXEC) {
+      setdt(1);
+      while (n++ < nmax && tim < tmax) {
+        one_step(h.flg, dts);
+        steps++;
+      }
+    } else {
+      ref_die("unknown mode");
+    }
+    *elapsed = omp_get_wtime() - t0;
+    return steps;
+  }
+  double time_now() const { return tim; }
+  double dt_now() const { return dt; }
+  double *const *state() const { return val; }
+  long cells() const { return (long)nd; }
+};
+
+int main(int argc, char **argv)
+{
+  if (argc != 3) ref_die("usage: ref3d <case.bin> <result.bin>");
+  RefCaseHeader h;
+  std::vector<double> data;
+  ref_read_case(argv[1], &h, &data);
+  if (h.dim != 3) ref_die("ref3d needs dim=3");
+  if (h.ctw != CTW) ref_die("binary built for the other CTW setting");
+  qh_xmesh = h.nxm; qh_ymesh = h.nym; qh_zmesh = h.nzm;
+  qh_rmn = h.rmn; qh_odr = h.odr; qh_rk = h.rk;
+  qh_cfl = h.cfl; qh_dtrec = h.dtrec; qh_nout = h.nout;
+  if (h.nthreads > 0) omp_set_num_threads(h.nthreads);
+
+  RefHarness3D *sim = new RefHarness3D(&argc, &argv);
+  sim->setup(h, data.data());
+  std::vector<double> dts;
+  double elapsed = 0.0;
+  int steps = sim->run(h, &dts, &elapsed);
+
+  RefResultHeader r;
+  memset(&r, 0, sizeof(r));
+  r.magic = QAS_REF_MAGIC_OUT;
+  r.nsteps_done = steps;
+  r.n_dt = (int)dts.size();
+  r.nd = (int)sim->cells();
+  r.tim = sim->time_now();
+  r.dt = sim->dt_now();
+  r.elapsed_s = elapsed;
+  ref_write_result(argv[2], r, dts, sim->state(), r.nd);
+  delete sim;
+  return 0;
+}

@@ -1,0 +1,81 @@
+/*
+ * Binary case format shared by the reference harnesses (oracle/_ref/*) and the
+ * Python test helpers (qasmhd oracle tooling in tests/).  Test infrastructure.
+ *
+ * Input  : RefCaseHeader, then 8 arrays (ro,mx,my,mz,bx,by,bz,en) of nd doubles,
+ *          each in the reference layout ss = nx*(ny*k+j)+i with 4 ghost cells
+ *          per side (2D/SERIAL/OTvortex/mhd2d_class.hpp:10-12).
+ * Output : RefResultHeader, n_dt doubles (dt used by each step), then the 8
+ *          arrays after the run.
+ */
+#ifndef QAS_REF_IO_H
+#define QAS_REF_IO_H
+
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+
+#define QAS_REF_MAGIC_IN  0x31534151   /* "QAS1" */
+#define QAS_REF_MAGIC_OUT 0x32534151   /* "QAS2" */
+
+enum RefMode {
+  REF_MODE_STEP = 0,   /* bound(val); ideal(dt) once, with the given dt            */
+  REF_MODE_RUN  = 1,   /* setdt(1); nsteps x { tim+=dt; bound; ideal; setdt(flg) } */
+  REF_MODE_EXEC = 2,   /* exec_(flg) loop termination: n<nmax && tim<tmax          */
+  REF_MODE_DRUN = 3,   /* RUN with the dissipative sub-cycle after ideal (2D only) */
+  REF_MODE_DSTEP = 4   /* bound; dsptv(dt) once (2D only)                          */
+};
+
+#pragma pack(push, 1)
+struct RefCaseHeader {
+  int32_t magic;
+  int32_t dim, nxm, nym, nzm;
+  int32_t rmn, odr, rk, ctw;
+  int32_t mode, nsteps, flg, nthreads;
+  int32_t nout, pad0;
+  double gam, cfl, dtrec, dt;
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double nu0, eta0;
+  int32_t dnx[8], dny[8], dnz[8];
+};
+struct RefResultHeader {
+  int32_t magic, nsteps_done, n_dt, nd;
+  double tim, dt, elapsed_s, pad;
+};
+#pragma pack(pop)
+
+static inline void ref_die(const char *msg)
+{
+  fprintf(stderr, "qas ref harness: %s\n", msg);
+  exit(2);
+}
+
+static inline void ref_read_case(const char *path, RefCaseHeader *h, std::vector<double> *data)
+{
+  FILE *f = fopen(path, "rb");
+  if (!f) ref_die("cannot open input");
+  if (fread(h, sizeof(*h), 1, f) != 1) ref_die("short header");
+  if (h->magic != QAS_REF_MAGIC_IN) ref_die("bad magic");
+  long nx = h->nxm + 8;
+  long ny = h->dim >= 2 ? h->nym + 8 : 1;
+  long nz = h->dim >= 3 ? h->nzm + 8 : 1;
+  size_t n = (size_t)(8 * nx * ny * nz);
+  data->resize(n);
+  if (fread(data->data(), sizeof(double), n, f) != n) ref_die("short data");
+  fclose(f);
+}
+
+static inline void ref_write_result(const char *path, const RefResultHeader &r,
+                                    const std::vector<double> &dts, double *const val[8], long nd)
+{
+  FILE *f = fopen(path, "wb");
+  if (!f) ref_die("cannot open output");
+  fwrite(&r, sizeof(r), 1, f);
+  if (!dts.empty()) fwrite(dts.data(), sizeof(double), dts.size(), f);
+  for (int m = 0; m < 8; m++) fwrite(val[m], sizeof(double), (size_t)nd, f);
+  fclose(f);
+}
+
+#endif

@@ -1,0 +1,238 @@
+"""Drivers for the CPU oracles (test infrastructure; never used by the product).
+
+* ``run_reference``: writes a case file, runs the reference's own stepping code
+  compiled from its sources (``oracle/_ref/ref{1,2,3}d*``, built by
+  ``oracle/Makefile`` with the reference flags -O2 -fopenmp) and reads back
+  the state and the dt sequence.
+* ``run_kat``: point-function known answers from ``oracle/_ref/ref_kat``.
+* ``Restatement``: ctypes binding of ``oracle/liboracle_qas.so``, our plain-C
+  restatement of the same algorithm (``oracle/qas_oracle.c``).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+import tempfile
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+LIB_PATH = os.path.join(HERE, "liboracle_qas.so")
+
+MODE_STEP, MODE_RUN, MODE_EXEC, MODE_DRUN, MODE_DSTEP = 0, 1, 2, 3, 4
+
+_HDR = struct.Struct("<15i12d24i")
+_RES = struct.Struct("<4i4d")
+MAGIC_IN = 0x31534151
+MAGIC_OUT = 0x32534151
+
+
+def ref_binary(dim: int, ctw: int) -> str:
+    name = "ref1d" if dim == 1 else f"ref{dim}d_ctw{int(bool(ctw))}"
+    return os.path.join(REF_DIR, name)
+
+
+def reference_available(dim: int = 2, ctw: int = 1) -> bool:
+    return os.access(ref_binary(dim, ctw), os.X_OK)
+
+
+def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nthreads: int = 0,
+               state: Optional[np.ndarray] = None) -> None:
+    st = prob.state if state is None else state
+    st = np.ascontiguousarray(st, dtype=np.float64).reshape(8, -1)
+    assert st.shape[1] == prob.nd, (st.shape, prob.nd)
+    hdr = _HDR.pack(MAGIC_IN, prob.dim, prob.nxm, prob.nym, prob.nzm,
+                    prob.rmn, prob.odr, prob.rk, prob.ctw,
+                    mode, nsteps, prob.flg, nthreads, prob.nout, 0,
+                    prob.gam, prob.cfl, prob.dtrec, dt,
+                    prob.xmin, prob.xmax, prob.ymin, prob.ymax, prob.zmin, prob.zmax,
+                    prob.nu0, prob.eta0,
+                    *[int(v) for v in prob.dnx], *[int(v) for v in prob.dny], *[int(v) for v in prob.dnz])
+    with open(path, "wb") as f:
+        f.write(hdr)
+        f.write(st.tobytes())
+
+
+def read_result(path: str, prob):
+    with open(path, "rb") as f:
+        raw = f.read()
+    magic, steps, ndt, nd, tim, dt, elapsed, _ = _RES.unpack_from(raw, 0)
+    assert magic == MAGIC_OUT
+    off = _RES.size
+    dts = np.frombuffer(raw, dtype=np.float64, count=ndt, offset=off).copy()
+    off += 8 * ndt
+    st = np.frombuffer(raw, dtype=np.float64, count=8 * nd, offset=off).copy()
+    st = st.reshape(8, prob.nz, prob.ny, prob.nx)
+    return {"state": st, "dts": dts, "steps": steps, "tim": tim, "dt": dt, "elapsed": elapsed}
+
+
+def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
+                  state: Optional[np.ndarray] = None, timeout: float = 3600.0):
+    """Run the reference's own code on ``prob`` and return its result dict."""
+    exe = ref_binary(prob.dim, prob.ctw)
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError(f"reference oracle binary missing: {exe} (build with `make -C oracle ref`)")
+    with tempfile.TemporaryDirectory(prefix="qasref_") as td:
+        cin = os.path.join(td, "case.bin")
+        cout = os.path.join(td, "result.bin")
+        write_case(cin, prob, mode, nsteps=nsteps, dt=dt, nthreads=nthreads, state=state)
+        env = dict(os.environ)
+        if nthreads > 0:
+            env["OMP_NUM_THREADS"] = str(nthreads)
+        subprocess.run([exe, cin, cout], check=True, env=env, timeout=timeout,
+                       stdout=subprocess.DEVNULL)
+        return read_result(cout, prob)
+
+
+def run_kat(func: int, inputs: np.ndarray, nout: int) -> np.ndarray:
+    exe = os.path.join(REF_DIR, "ref_kat")
+    inputs = np.ascontiguousarray(inputs, dtype=np.float64)
+    ncase, nin = inputs.shape
+    with tempfile.TemporaryDirectory(prefix="qaskat_") as td:
+        cin = os.path.join(td, "in.bin")
+        cout = os.path.join(td, "out.bin")
+        with open(cin, "wb") as f:
+            f.write(struct.pack("<4i", func, ncase, nin, nout))
+            f.write(inputs.tobytes())
+        subprocess.run([exe, cin, cout], check=True, stdout=subprocess.DEVNULL)
+        return np.fromfile(cout, dtype=np.float64).reshape(ncase, nout)
+
+
+# ---------------------------------------------------------------------------
+# ctypes binding of the plain-C restatement
+# ---------------------------------------------------------------------------
+
+class _OGrid(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("nxm", ctypes.c_int), ("nym", ctypes.c_int),
+                ("nzm", ctypes.c_int), ("rmn", ctypes.c_int), ("odr", ctypes.c_int),
+                ("rk", ctypes.c_int), ("ctw", ctypes.c_int),
+                ("gam", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("dz", ctypes.c_double),
+                ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8)]
+
+
+class Restatement:
+    """The plain-C oracle (oracle/qas_oracle.c) driven through ctypes."""
+
+    def __init__(self, path: str = LIB_PATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (build with `make -C oracle oracle`)")
+        self.lib = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        self.lib.qo_step.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double]
+        self.lib.qo_step.restype = ctypes.c_int
+        self.lib.qo_bound.argtypes = [ctypes.POINTER(_OGrid), dp]
+        self.lib.qo_bound.restype = None
+        self.lib.qo_cfl_dt.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double]
+        self.lib.qo_cfl_dt.restype = ctypes.c_double
+        self.lib.qo_dissipate.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double]
+        self.lib.qo_dissipate.restype = ctypes.c_int
+        self.lib.qo_dsptv.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double]
+        self.lib.qo_dsptv.restype = ctypes.c_int
+        self.lib.qo_kat.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
+        self.lib.qo_kat.restype = ctypes.c_int
+
+    @staticmethod
+    def grid(prob) -> _OGrid:
+        g = _OGrid()
+        g.dim, g.nxm, g.nym, g.nzm = prob.dim, prob.nxm, prob.nym, prob.nzm
+        g.rmn, g.odr, g.rk, g.ctw = prob.rmn, prob.odr, prob.rk, prob.ctw
+        g.gam, g.dx = prob.gam, prob.dx
+        g.dy = prob.dy if prob.dim >= 2 else 0.0
+        g.dz = prob.dz if prob.dim >= 3 else 0.0
+        for m in range(8):
+            g.dnx[m], g.dny[m], g.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+        return g
+
+    @staticmethod
+    def _ptr(a: np.ndarray):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    def dr(self, prob) -> float:
+        d = [prob.dx]
+        if prob.dim >= 2:
+            d.append(prob.dy)
+        if prob.dim >= 3:
+            d.append(prob.dz)
+        r = d[0]
+        for v in d[1:]:
+            r = v if r >= v else r   # min() of common/common_func.h:11-15
+        return r
+
+    def run(self, prob, nsteps: int, state: Optional[np.ndarray] = None, mode: int = MODE_RUN,
+            dt: float = 0.0):
+        """Same semantics as :func:`run_reference` for MODE_STEP/RUN/EXEC/DRUN/DSTEP."""
+        g = self.grid(prob)
+        st = np.ascontiguousarray((prob.state if state is None else state), dtype=np.float64).copy()
+        p = self._ptr(st)
+        dts = []
+        dr = self.dr(prob)
+        if mode == MODE_STEP:
+            self.lib.qo_bound(ctypes.byref(g), p)
+            rc = self.lib.qo_step(ctypes.byref(g), p, dt)
+            assert rc == 0
+            return {"state": st, "dts": np.array([dt]), "steps": 1, "tim": dt, "dt": dt}
+        if mode == MODE_DSTEP:
+            self.lib.qo_bound(ctypes.byref(g), p)
+            rc = self.lib.qo_dsptv(ctypes.byref(g), p, dt, prob.nu0, prob.eta0)
+            assert rc == 0
+            return {"state": st, "dts": np.array([dt]), "steps": 1, "tim": dt, "dt": dt}
+        # setdt(1): CFL dt and nmax from the first dt (mhd2d_class.cpp:11-33)
+        vmax = self.lib.qo_cfl_dt(ctypes.byref(g), p, 1.0)
+        dt = prob.cfl * (dr if prob.dim > 1 else prob.dx) / vmax
+        if prob.dim == 1:
+            nrec = int(prob.dtrec / dt + 0.5)
+            nmax = nrec * prob.nout
+        else:
+            nmax = int(prob.tmax / dt + 0.5)
+        tim = 0.0
+        n = 0
+        steps = 0
+
+        def one(n_now):
+            nonlocal tim, dt
+            tim += dt
+            dts.append(dt)
+            self.lib.qo_bound(ctypes.byref(g), p)
+            rc = self.lib.qo_step(ctypes.byref(g), p, dt)
+            assert rc == 0
+            if mode == MODE_DRUN:
+                rc = self.lib.qo_dissipate(ctypes.byref(g), p, dt, prob.nu0, prob.eta0)
+                assert rc == 0
+            if prob.flg * (n_now % 2 == 0):
+                vm = self.lib.qo_cfl_dt(ctypes.byref(g), p, 1.0)
+                dt = prob.cfl * (dr if prob.dim > 1 else prob.dx) / vm
+
+        if mode in (MODE_RUN, MODE_DRUN):
+            for _ in range(nsteps):
+                n += 1
+                one(n)
+                steps += 1
+        elif mode == MODE_EXEC:
+            while True:
+                cond = (n < nmax and tim < prob.tmax) if (prob.flg or prob.dim > 1) else (n < nmax)
+                n += 1
+                if not cond:
+                    break
+                one(n)
+                steps += 1
+        else:
+            raise ValueError(mode)
+        return {"state": st, "dts": np.array(dts), "steps": steps, "tim": tim, "dt": dt}
+
+    def kat(self, func: int, inputs: np.ndarray, nout: int) -> np.ndarray:
+        inputs = np.ascontiguousarray(inputs, dtype=np.float64)
+        ncase, nin = inputs.shape
+        out = np.zeros((ncase, nout), dtype=np.float64)
+        rc = self.lib.qo_kat(func, ncase, nin, nout, self._ptr(inputs), self._ptr(out))
+        assert rc == 0, f"qo_kat({func}) failed"
+        return out

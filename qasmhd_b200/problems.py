@@ -1,0 +1,296 @@
+"""Initial states and run settings for the qasMHD problems this library steps.
+
+A :class:`Problem` carries everything the reference fixes per problem
+directory: the compile-time settings of ``mymacros.hpp`` (grid size, Riemann
+solver ``rmn``, spatial order ``odr``, Runge-Kutta order ``rk``, CUCT weighting
+``ctw``, CFL, output cadence; e.g. 2D/SERIAL/OTvortex/mymacros.hpp:4-14), the
+run-time settings of ``paras()`` (domain, boundary flags ``dnxs/dnys/dnzs``,
+gamma; 2D/SERIAL/OTvortex/mhd2d_paras.cpp:3-39) and the conservative state that
+``init_()`` leaves behind (ro,mx,my,mz,bx,by,bz,en with 4 ghost cells per side,
+ss = nx*(ny*k+j)+i; common/mhd_class.hpp:32-42).
+
+Boundary flags follow the reference (common/common_func.h:256-271):
+0 periodic, +1 Neumann, -1 Dirichlet, +2 open, -2 zero-fixed.
+
+Everything here is host-side numpy; the state goes to the device through the
+C-ABI (``qasmhd_b200.lib``).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional, Sequence
+
+import numpy as np
+
+XOFF = 4  # ghost cells per side (2D/SERIAL/OTvortex/mhd2d_class.hpp:10-12)
+NM = 8    # number of MHD variables (common/mhd_class.hpp:17)
+
+RMN_ROE, RMN_HLLD, RMN_LHLLD, RMN_MLAU = 0, 1, 2, 3
+
+
+@dataclasses.dataclass
+class Problem:
+    """One simulation: grid, scheme, boundaries and the initial state."""
+
+    name: str
+    dim: int
+    nxm: int
+    nym: int = 1
+    nzm: int = 1
+    rmn: int = RMN_HLLD
+    odr: int = 4
+    rk: int = 3
+    ctw: int = 1
+    gam: float = 5.0 / 3.0
+    cfl: float = 0.4
+    dtrec: float = 1.0
+    nout: int = 1
+    xmin: float = 0.0
+    xmax: float = 1.0
+    ymin: float = 0.0
+    ymax: float = 1.0
+    zmin: float = 0.0
+    zmax: float = 1.0
+    dnx: Sequence[int] = (0,) * NM
+    dny: Sequence[int] = (0,) * NM
+    dnz: Sequence[int] = (0,) * NM
+    nu0: float = 0.0
+    eta0: float = 0.0
+    # exec_ flag: 1 = dt refreshed every 2nd step (2D/3D drivers), 0 = constant dt (1D driver)
+    flg: int = 1
+    state: Optional[np.ndarray] = None  # shape (8, nz, ny, nx) incl. ghosts
+
+    @property
+    def nx(self) -> int:
+        return self.nxm + 2 * XOFF
+
+    @property
+    def ny(self) -> int:
+        return self.nym + 2 * XOFF if self.dim >= 2 else 1
+
+    @property
+    def nz(self) -> int:
+        return self.nzm + 2 * XOFF if self.dim >= 3 else 1
+
+    @property
+    def nd(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def interior_cells(self) -> int:
+        return self.nxm * (self.nym if self.dim >= 2 else 1) * (self.nzm if self.dim >= 3 else 1)
+
+    @property
+    def dx(self) -> float:
+        return (self.xmax - self.xmin) / self.nxm
+
+    @property
+    def dy(self) -> float:
+        return (self.ymax - self.ymin) / self.nym
+
+    @property
+    def dz(self) -> float:
+        return (self.zmax - self.zmin) / self.nzm
+
+    @property
+    def tmax(self) -> float:
+        return self.dtrec * self.nout
+
+    def coords(self):
+        """Cell-centre coordinates incl. ghosts, (i-xoff+0.5)*dx+xmin as in
+        2D/SERIAL/KHI/mhd2d_paras.cpp:36-37."""
+        x = (np.arange(self.nx) - XOFF + 0.5) * self.dx + self.xmin
+        y = (np.arange(self.ny) - XOFF + 0.5) * self.dy + self.ymin if self.dim >= 2 else np.zeros(1)
+        z = (np.arange(self.nz) - XOFF + 0.5) * self.dz + self.zmin if self.dim >= 3 else np.zeros(1)
+        return x, y, z
+
+    def copy(self) -> "Problem":
+        p = dataclasses.replace(self)
+        p.state = None if self.state is None else self.state.copy()
+        return p
+
+
+def _energy(ro, vx, vy, vz, bx, by, bz, pr, gam):
+    """Total energy, same expression order as mhd_energy (common/mhd_func.c:18-28)."""
+    v2 = vx * vx + vy * vy + vz * vz
+    b2 = bx * bx + by * by + bz * bz
+    return pr / (gam - 1) + 0.5 * (ro * v2 + b2)
+
+
+def _pack(ro, vx, vy, vz, bx, by, bz, pr, cx, cy, cz, gam):
+    """Primitive -> conservative (cnsvt, common/mhd_class.hpp:73-79); B energy
+    uses the cell-centre field cx,cy,cz."""
+    st = np.empty((NM,) + ro.shape, dtype=np.float64)
+    st[0] = ro
+    st[1] = ro * vx
+    st[2] = ro * vy
+    st[3] = ro * vz
+    st[4] = bx
+    st[5] = by
+    st[6] = bz
+    st[7] = _energy(ro, vx, vy, vz, cx, cy, cz, pr, gam)
+    return st
+
+
+def _df(f0m1, f0, f1, f2, odr):
+    """df1[ODR-1] on four consecutive values (common/common_interp.h:17-24)."""
+    if odr >= 3:
+        return (27.0 * (f1 - f0) - (f2 - f0m1)) / 24.0
+    return f1 - f0
+
+
+# ----------------------------------------------------------------------------
+# C1: Brio-Wu shock tube
+# ----------------------------------------------------------------------------
+
+def brio_wu(nxm: int = 1024, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3,
+            tmax: float = 0.1) -> Problem:
+    """Brio & Wu shock tube on x in [0,1], outflow boundaries, gamma=2.
+
+    Left (ro,pr,vx,vy,vz,bx,by,bz)=(1,1,0,0,0,0.75,1,0), right
+    (0.125,0.1,0,0,0,0.75,-1,0); discontinuity at x=0.5 (the reference puts the
+    same states on [-0.5,0.5] split at x<=0, 1D/SERIAL/shock/mhd1d_init_.cpp:14-30).
+    The 1D driver runs with a constant dt (exec_(0), 1D/SERIAL/shock/main.cpp).
+    """
+    p = Problem(name=f"briowu_{nxm}", dim=1, nxm=nxm, rmn=rmn, odr=odr, rk=rk, ctw=0,
+                gam=2.0, cfl=0.4, dtrec=tmax, nout=1, xmin=0.0, xmax=1.0,
+                dnx=(2,) * NM, flg=0)
+    x, _, _ = p.coords()
+    left = x <= 0.5
+    ro = np.where(left, 1.0, 0.125)
+    pr = np.where(left, 1.0, 0.1)
+    z = np.zeros_like(x)
+    bx = np.full_like(x, 0.75)
+    by = np.where(left, 1.0, -1.0)
+    st = _pack(ro, z, z, z, bx, by, z, pr, bx, by, z, p.gam)
+    p.state = st.reshape(NM, 1, 1, p.nx)
+    return p
+
+
+# ----------------------------------------------------------------------------
+# C2: Orszag-Tang vortex
+# ----------------------------------------------------------------------------
+
+def orszag_tang(n: int = 1024, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3, ctw: int = 1,
+                tmax: float = 0.5, nym: Optional[int] = None) -> Problem:
+    """Orszag-Tang vortex on [0,2pi]^2, periodic, gamma=5/3.
+
+    ro=25/(36pi), pr=5/(12pi), v=(-sin y, sin x, 0),
+    B=(-sin y, sin 2x, 0)/sqrt(4pi) built on the faces from the corner vector
+    potential A_z=(cos y + cos(2x)/2)/sqrt(4pi) with the same difference
+    operator df1[ODR-1] the CT update uses (the idiom of
+    2D/SERIAL/loop/mhd2d_init_.cpp:22-55), so the ODR-consistent div B is zero.
+    """
+    nym = n if nym is None else nym
+    p = Problem(name=f"ot_{n}x{nym}", dim=2, nxm=n, nym=nym, rmn=rmn, odr=odr, rk=rk, ctw=ctw,
+                gam=5.0 / 3.0, cfl=0.4, dtrec=tmax, nout=1,
+                xmin=0.0, xmax=2.0 * math.pi, ymin=0.0, ymax=2.0 * math.pi, flg=1)
+    x, y, _ = p.coords()
+    dx, dy = p.dx, p.dy
+    s4 = math.sqrt(4.0 * math.pi)
+    X, Y = np.meshgrid(x, y)  # (ny, nx)
+    # corner potential at (x-dx/2, y-dy/2), one extra ring for the 4-point stencils
+    xc = (np.arange(-1, p.nx + 2) - XOFF) * dx + p.xmin
+    yc = (np.arange(-1, p.ny + 2) - XOFF) * dy + p.ymin
+    XC, YC = np.meshgrid(xc, yc)
+    az = (np.cos(YC) + 0.5 * np.cos(2.0 * XC)) / s4        # index [j+1, i+1] <-> corner (i-1/2, j-1/2)
+    # bx at face (i-1/2, j) = +D_y A over corners j-3/2..j+3/2 (rows j..j+3 of az)
+    bx = _df(az[0:-3, 1:-2], az[1:-2, 1:-2], az[2:-1, 1:-2], az[3:, 1:-2], odr) / dy
+    by = -_df(az[1:-2, 0:-3], az[1:-2, 1:-2], az[1:-2, 2:-1], az[1:-2, 3:], odr) / dx
+    ro = np.full_like(X, 25.0 / (36.0 * math.pi))
+    pr = np.full_like(X, 5.0 / (12.0 * math.pi))
+    vx = -np.sin(Y)
+    vy = np.sin(X)
+    z = np.zeros_like(X)
+    cx = -np.sin(Y) / s4
+    cy = np.sin(2.0 * X) / s4
+    st = _pack(ro, vx, vy, z, bx, by, z, pr, cx, cy, z, p.gam)
+    p.state = st.reshape(NM, 1, p.ny, p.nx)
+    return p
+
+
+# ----------------------------------------------------------------------------
+# C3/C4/C5: Kelvin-Helmholtz
+# ----------------------------------------------------------------------------
+
+def kelvin_helmholtz(dim: int = 3, n: int = 256, mach: float = 0.01, beta: float = 100.0,
+                     rmn: int = RMN_MLAU, odr: int = 4, rk: int = 3, ctw: int = 1,
+                     gam: float = 5.0 / 3.0, seed: int = 12345, nym: Optional[int] = None,
+                     nzm: Optional[int] = None, noise: float = 1e-3, tmax: float = 1e30,
+                     nout: int = 1, dvy_field: Optional[np.ndarray] = None) -> Problem:
+    """Low-Mach Kelvin-Helmholtz layer on [-0.5,0.5]^dim.
+
+    Periodic in x (and z), open (+2) in y.  vx=(M/2) tanh(y/0.05) with sonic Mach
+    M (sound speed 1: ro=1, pr=1/gam), uniform guide field bz giving plasma
+    beta=2pr/B^2, weak bx=0.01.  Gaussian velocity perturbations of amplitude
+    noise*M localised by exp(-(y/0.1)^2) come from numpy's default_rng(seed),
+    so both codes receive the identical state.  ``dvy_field`` (interior-shaped)
+    replaces the random vy perturbation (used by the gradient tests).
+    """
+    nym = n if nym is None else nym
+    nzm = (n if nzm is None else nzm) if dim >= 3 else 1
+    dn_y = (2,) * NM
+    p = Problem(name=f"kh{dim}d_{n}", dim=dim, nxm=n, nym=nym, nzm=nzm, rmn=rmn, odr=odr, rk=rk,
+                ctw=ctw, gam=gam, cfl=0.4, dtrec=tmax, nout=nout,
+                xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5,
+                zmin=-0.5, zmax=0.5, dnx=(0,) * NM, dny=dn_y, dnz=(0,) * NM, flg=1)
+    x, y, z = p.coords()
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")  # (nz, ny, nx)
+    rng = np.random.default_rng(seed)
+    amp = noise * mach * np.exp(-(Y / 0.1) ** 2)
+    shape = X.shape
+    ro = np.ones(shape)
+    pr = np.full(shape, 1.0 / gam)
+    vx = 0.5 * mach * np.tanh(Y / 0.05) + amp * rng.standard_normal(shape)
+    if dvy_field is not None:
+        full = np.zeros(shape)
+        sl = (slice(XOFF, XOFF + nzm) if dim >= 3 else slice(0, 1),
+              slice(XOFF, XOFF + nym), slice(XOFF, XOFF + p.nxm))
+        full[sl] = np.asarray(dvy_field, dtype=np.float64).reshape(full[sl].shape)
+        vy = amp * full
+        rng.standard_normal(shape)
+    else:
+        vy = amp * rng.standard_normal(shape)
+    vz = amp * rng.standard_normal(shape) if dim >= 3 else np.zeros(shape)
+    bx = np.full(shape, 0.01)
+    by = np.zeros(shape)
+    bz = np.full(shape, math.sqrt(2.0 * (1.0 / gam) / beta))
+    st = _pack(ro, vx, vy, vz, bx, by, bz, pr, bx, by, bz, gam)
+    p.state = st
+    return p
+
+
+def smooth_wave(dim: int, n: int, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3, ctw: int = 1,
+                seed: int = 7, amp: float = 1e-2, dn=None) -> Problem:
+    """Small random smooth perturbation of a uniform magnetised plasma; periodic
+    unless ``dn`` gives per-axis flag tuples.  Used by parity tests to exercise
+    every solver/BC combination on small grids."""
+    rng = np.random.default_rng(seed)
+    nyz = n if dim >= 2 else 1
+    p = Problem(name=f"wave{dim}d_{n}", dim=dim, nxm=n, nym=nyz, nzm=n if dim >= 3 else 1,
+                rmn=rmn, odr=odr, rk=rk, ctw=ctw, gam=5.0 / 3.0, cfl=0.4,
+                xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0, flg=1)
+    if dn is not None:
+        p.dnx, p.dny, p.dnz = dn
+    shape = (p.nz, p.ny, p.nx)
+    x, y, z = p.coords()
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    ph = rng.uniform(0, 2 * np.pi, size=8)
+
+    def wave(k):
+        return np.sin(2 * np.pi * X + ph[k]) * np.cos(2 * np.pi * (Y + Z) + ph[k])
+
+    ro = 1.0 + amp * wave(0)
+    vx = 0.3 + amp * wave(1)
+    vy = -0.2 + amp * wave(2)
+    vz = 0.1 + amp * wave(3)
+    bx = 0.7 + amp * wave(4)
+    by = 0.4 + amp * wave(5)
+    bz = -0.3 + amp * wave(6)
+    pr = 0.8 + amp * wave(7)
+    if dim < 3:
+        vz = vz * 1.0
+    st = _pack(ro, vx, vy, vz, bx, by, bz, pr, bx, by, bz, p.gam)
+    p.state = st
+    return p
