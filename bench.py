@@ -1,0 +1,261 @@
+"""Benchmark: qasMHD per-step update in Mcell-updates/s (FP64) on B200.
+
+Default workload (N=1): 2D Orszag-Tang vortex 1024^2, HLLD + characteristic
+WCNS4 + CUCT-weighted CT + SSP-RK3, CFL 0.4, dt refreshed every 2nd step as in
+exec_.  One "step" = one full RK3 time step of the whole grid.  Under torchrun
+(N>1) every rank advances its own independent replica (the plain path is a
+single domain; replicas only), so per-GPU work is fixed: weak scaling.
+
+--impl reference runs the reference's own OpenMP code, compiled from its
+sources (oracle/_ref), on the host cores for the same workload.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+ALG_BYTES_PER_CELL_UPDATE = 512  # 8 FP64 fields: stage 1 reads u^n, writes; stages 2-3 read stage input + u^n, write
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "bw1d_1024"], default="ot2d_1024")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=6)
+    return ap.parse_args()
+
+
+def make_problem(name):
+    from qasmhd_b200 import problems as P
+    if name == "ot2d_1024":
+        p = P.orszag_tang(1024)
+        cfg = {"workload": "orszag_tang_2d_1024x1024", "grid": [1024, 1024], "solver": "HLLD", "order": "WCNS4",
+               "rk": 3, "ct": "CUCT", "bc": "periodic", "gamma": "5/3"}
+    elif name == "kh3d_256":
+        p = P.kelvin_helmholtz(3, 256)
+        cfg = {"workload": "kelvin_helmholtz_3d_256^3", "grid": [256, 256, 256], "solver": "MLAU",
+               "order": "WCNS4", "rk": 3, "ct": "CUCT", "bc": "periodic x,z / open y", "mach": 0.01, "beta": 100}
+    else:
+        p = P.brio_wu(1024)
+        cfg = {"workload": "brio_wu_1d_1024", "grid": [1024], "solver": "HLLD", "order": "WCNS4", "rk": 3}
+    return p, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline(prob, steps=3, threads=None):
+    """The reference's own OpenMP code (oracle/_ref) on a bounded sample of the workload."""
+    from oracle import refcase as R
+    threads = threads or os.cpu_count()
+    if not R.reference_available(prob.dim, prob.ctw):
+        return None
+    r = R.run_reference(prob, R.MODE_RUN, nsteps=steps, nthreads=threads)
+    st = r["step_times"]
+    per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
+    return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, "
+                      f"reference -O2 -fopenmp, OMP_NUM_THREADS={threads}"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    prob, cfg = make_problem(args.workload)
+    if rank != 0:
+        return
+    from oracle import refcase as R
+    threads = os.cpu_count()
+    if not R.reference_available(prob.dim, prob.ctw):
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle binaries (oracle/_ref) not built"}))
+        return
+    r = R.run_reference(prob, R.MODE_RUN, nsteps=args.warmup + args.steps, nthreads=threads)
+    st = r["step_times"][args.warmup:]
+    total = float(np.sum(st))
+    value = prob.interior_cells * len(st) / total / 1e6
+    line = {"metric": "Mcell-updates/s/GPU FP64 (per-step update)", "value": value, "unit": "Mcell-updates/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": len(st), "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / len(st), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial state of the named problem)",
+            "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
+                             "sample": f"{prob.name}: {args.warmup}+{len(st)} steps, reference -O2 -fopenmp"},
+            "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from qasmhd_b200 import lib as L
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    prob, cfg = make_problem(args.workload)
+    cells = prob.interior_cells
+    ctx = L.Context.from_problem(prob, device=local)
+    ctx.upload(prob.state)
+    ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (includes setdt(1) and the graph capture)
+    ctx.run(max_steps=args.warmup, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ctx.kernel_launches()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(ext)
+    ctx.run(max_steps=args.steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+    end.record(ext)
+    end.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.kernel_launches() - l0
+    ms = start.elapsed_time(end)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = cells * args.steps * world / (ms_max * 1e-3) / 1e6
+
+    # end-to-end through the public API with pinned host buffers: every step uploads the
+    # state, advances one exec_ step and downloads the state (the drop-in for ideal() on
+    # host arrays)
+    host = torch.empty((8, prob.nd), dtype=torch.float64, pin_memory=True)
+    host.copy_(torch.from_numpy(np.ascontiguousarray(prob.state).reshape(8, -1)))
+    hptr = host.numpy()
+    nb = hptr.nbytes
+    barrier()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(ext)
+    for _ in range(args.e2e_steps):
+        ctx.upload(hptr)
+        ctx.run(max_steps=1, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=False)
+        ctx.download_into(hptr)
+    e_end.record(ext)
+    e_end.synchronize()
+    barrier()
+    e_ms = e_start.elapsed_time(e_end)
+    te = torch.tensor([e_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e_value = cells * args.e2e_steps * world / (float(te.item()) * 1e-3) / 1e6
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = ALG_BYTES_PER_CELL_UPDATE * cells / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": "Mcell-updates/s/GPU FP64 (per-step update)", "value": value, "unit": "Mcell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded initial state of the named problem)",
+        "config": dict(cfg, parallelism=f"replicas{world}",
+                       l2="working set per step ~%.2f GB > 126 MB L2" % (77 * prob.nd * 8 / 1e9)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None,
+                     "basis": "whole step, 512 algorithmic B per cell-update, peak of measured"},
+        "e2e": {"value": e_value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(prob)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+/*
+ * qas.h -- C-ABI of libqas, the B200 (sm_100a) FP64 implementation of
+ * qasMHD's per-step update.
+ *
+ * The reference exposes this path as non-virtual members of its dimension
+ * classes (MHD1D / MHD2D / MHD3D, plus DMHD2D for the visco-resistive form)
+ * operating in place on caller-owned host arrays in the layout
+ *   val[m][ss], m = ro,mx,my,mz,bx,by,bz,en, ss = nx*(ny*k+j)+i,
+ *   nx = XMESH+8 (4 ghost cells per side), bx/by/bz on the lower faces
+ * (common/mhd_class.hpp:32-42, 2D/SERIAL/OTvortex/mhd2d_class.cpp:116-164).
+ * Each entry point below names the reference member it replaces.
+ *
+ * Conventions
+ *  - Every call returns qas_status; QAS_OK == 0.  No C++ exception crosses the ABI.
+ *  - A context owns its device buffers and one CUDA stream on one device; calls on
+ *    one context must come from one host thread at a time.  Distinct contexts are
+ *    independent.
+ *  - Host arrays stay owned by the caller.  Upload/download are synchronous.
+ *  - Results are bit-identical to the reference CPU build for the same inputs.
+ *  - Device-detected failures (non-positive density, non-finite values, a bounded
+ *    device wait that ran out) latch in the context and are returned by the next call
+ *    that synchronises (qas_sync, downloads, qas_run).
+ */
+#ifndef QAS_H
+#define QAS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QAS_ABI_VERSION 1
+
+typedef enum {
+  QAS_OK = 0,
+  QAS_ERR_INVALID = 1,      /* bad argument (sizes, flags, null pointers)            */
+  QAS_ERR_CUDA = 2,         /* CUDA runtime error (see qas_last_cuda_error)          */
+  QAS_ERR_NOMEM = 3,        /* device allocation failed                              */
+  QAS_ERR_NONFINITE = 4,    /* device check found rho<=0, p<=0 or a non-finite value */
+  QAS_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up                    */
+  QAS_ERR_UNSUPPORTED = 6,  /* combination not implemented                           */
+  QAS_ERR_NO_DEVICE = 7     /* no usable CUDA device                                 */
+} qas_status;
+
+/* Grid: compile-time XMESH/YMESH/ZMESH of mymacros.hpp plus paras()'s spacing and gamma
+ * (2D/SERIAL/OTvortex/mymacros.hpp:4-8, mhd2d_paras.cpp:3-39, common/mhd_class.hpp:20-24). */
+typedef struct {
+  int dim;               /* 1, 2 or 3                                           */
+  int nxm, nym, nzm;     /* interior cells per axis (1 for unused axes)          */
+  double dx, dy, dz;     /* cell sizes (unused axes ignored)                     */
+  double gam;            /* specific-heat ratio (MHD::setgam)                    */
+} qas_grid;
+
+/* Scheme: RMN / ODR / R_K / CTW of mymacros.hpp (2D/SERIAL/OTvortex/mymacros.hpp:10-14).
+ *   rmn: 0 Roe, 1 HLLD, 2 LHLLD, 3 MLAU  (riemann[] order, common/mhd_class.hpp:102-105)
+ *   odr: 1..4 (interpol[ODR-1], l_interp, fcen, df1: common/mhd_class.hpp:107-113)
+ *   rk : 1..3 SSP Runge-Kutta stages (rk_fac, mhd2d_solve.cpp:7)
+ *   ctw: CUCT upwind weighting of the corner EMFs (mhd2d_solve.cpp:91-103) */
+typedef struct {
+  int rmn, odr, rk, ctw;
+} qas_scheme;
+
+/* Boundary flags per field and axis, the dnxs/dnys/dnzs arrays of common/mhd_class.hpp:40:
+ * 0 periodic, +1 Neumann, -1 Dirichlet, +2 open, -2 zero-fixed (common/common_func.h:256-271). */
+typedef struct {
+  int dnx[8], dny[8], dnz[8];
+} qas_bc;
+
+typedef struct qas_ctx qas_ctx;
+
+/* exec_() loop settings (mhd2d_class.cpp:35-61, mhd1d_class.cpp:32-53, mhd3d_class.cpp:48-76). */
+typedef struct {
+  int max_steps;     /* upper bound on steps taken by this call (<=0: no bound)                 */
+  int flg;           /* exec_ flag: 1 = refresh dt by setdt every 2nd step, 0 = constant dt      */
+  int stop_rule;     /* 0: run exactly max_steps; 1: exec_ rule n<nmax && tim<tmax (2D/3D);
+                        2: 1D rule n<nmax with nmax = nrec*nout (mhd1d_class.cpp:24-29)          */
+  double cfl;        /* CFL number (CFL macro)                                                   */
+  double dtrec;      /* DTREC macro                                                              */
+  int nout;          /* N_OUT macro; tmax = dtrec*nout                                           */
+  int use_graph;     /* capture the step loop in a CUDA graph                                    */
+  double nu0, eta0;  /* uniform viscosity / resistivity: when max(2nu0,eta0) > 1e-15 each step is
+                        followed by the sub-cycled dissipative update of DMHD2D::exec_ (2D only) */
+} qas_run_opts;
+
+typedef struct {
+  int steps;         /* steps taken by this call            */
+  int n;             /* exec_'s step counter after the call  */
+  int nmax;          /* nmax fixed by the first setdt        */
+  double tim;        /* simulated time                       */
+  double dt;         /* current dt                           */
+} qas_run_info;
+
+/* Library / device */
+const char *qas_status_str(qas_status s);
+int qas_abi_version(void);
+const char *qas_last_cuda_error(void);
+
+/* Context lifecycle.  Replaces the MHD{1,2,3}D constructor's array allocation and the
+ * paras() settings (mhd2d_class.cpp:116-164, mhd2d_paras.cpp:3-39).  `device` < 0 uses
+ * the current device. */
+qas_status qas_create(qas_ctx **ctx, const qas_grid *grid, const qas_scheme *scheme, const qas_bc *bc, int device);
+qas_status qas_destroy(qas_ctx *ctx);
+
+/* Number of cells nd = nx*ny*nz including ghosts. */
+qas_status qas_cells(const qas_ctx *ctx, long long *nd);
+
+/* Copy the 8 host arrays val[0..7] (nd doubles each, reference layout incl. ghosts)
+ * to / from the device.  Replaces the host-resident state of common/mhd_class.hpp:32-42. */
+qas_status qas_upload(qas_ctx *ctx, double *const val[8]);
+qas_status qas_download(qas_ctx *ctx, double *val[8]);
+/* Same with one contiguous host block of 8*nd doubles (field m at block + m*nd). */
+qas_status qas_upload_block(qas_ctx *ctx, const double *block);
+qas_status qas_download_block(qas_ctx *ctx, double *block);
+/* Device address of the context's state block (8*nd doubles, field-major); valid until
+ * qas_destroy.  Lets device-resident callers (CUDA, PyTorch) share the state without copies. */
+qas_status qas_device_state(qas_ctx *ctx, double **d_block);
+/* The context's CUDA stream (cudaStream_t as void*). */
+qas_status qas_stream(qas_ctx *ctx, void **stream);
+
+/* Ghost fill of the 8 state fields: MHD2D::bound (mhd2d_class.cpp:3-9 -> bc2d,
+ * common/common_func.c:60-138); 1D bc1d (:34-58); 3D single-rank mpi_sdrv3d +
+ * mpi_x/y/zbc3d (mpi/common_mpi.c:198-525). */
+qas_status qas_bound(qas_ctx *ctx);
+
+/* One SSP-RK step of the ideal equations with the given dt, including the per-stage
+ * ghost fill: MHD1D/2D/3D::ideal(dt) (1D/SERIAL/shock/mhd1d_solve.cpp:3-124,
+ * 2D/SERIAL/OTvortex/mhd2d_solve.cpp:3-400, 3D/MPI/KHI/mhd3d_solve.cpp:3-729).
+ * Like the reference, it does not fill the ghosts first: call qas_bound before. */
+qas_status qas_step(qas_ctx *ctx, double dt);
+
+/* setdt's reduction vmax = max(1, max over the interior of |v| + c_f) and the CFL
+ * time step dt = cfl*dr/vmax (mhd2d_class.cpp:11-33, mhd1d_class.cpp:11-30,
+ * mhd3d_class.cpp:15-46). */
+qas_status qas_cfl_vmax(qas_ctx *ctx, double *vmax);
+qas_status qas_cfl_dt(qas_ctx *ctx, double cfl, double *dt);
+
+/* The exec_() stepping loop on the device: setdt(1) once (on the first call), then
+ * { tim += dt; bound; ideal(dt); [dissipative sub-cycles]; setdt(flg*(n%2==0)) } per step,
+ * with dt, tim, n and the stop test kept on the device (graph-captured when use_graph).
+ * Output files of dout_() are not written. */
+qas_status qas_run(qas_ctx *ctx, const qas_run_opts *opts, qas_run_info *info);
+/* Reset exec_'s counters (n = 0, tim = 0, setdt(1) pending) without touching the state. */
+qas_status qas_run_reset(qas_ctx *ctx);
+
+/* Visco-resistive update with uniform coefficients: DMHD2D::setdc + the sub-cycled
+ * dsptv of DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26, dmhd2d_solve.cpp:3-151).
+ * qas_dsptv is one dsptv(dt) call (no ghost fill before).  2D only. */
+qas_status qas_dissipate(qas_ctx *ctx, double dt, double nu0, double eta0);
+qas_status qas_dsptv(qas_ctx *ctx, double dt, double nu0, double eta0);
+
+/* max over the interior of |D_x bx + D_y by + D_z bz| with the ODR-consistent
+ * difference df1[ODR-1] (common/common_interp.h:17-24) scaled by 1/dx etc.; the CT
+ * update keeps it at round-off (the check of 2D/SERIAL/python/batch.py:126-131). */
+qas_status qas_max_divb(qas_ctx *ctx, double *maxdivb);
+
+/* Wait for the context's stream and report any latched device error. */
+qas_status qas_sync(qas_ctx *ctx);
+
+/* Host-only diagnostics (no device needed): the ghost-fill map that qas_create builds for
+ * group (0 state, 1 cell-centre B, 2 shock detector dv), field and axis.  src[i], fac[i]
+ * for i < n (n = the axis extent incl. ghosts): after all fill passes of that axis, cell i
+ * holds fac[i] * (value at src[i]).  Returns QAS_ERR_INVALID for flags the reference
+ * leaves unset. */
+qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int field, int axis, int *src,
+                      double *fac, int n);
+
+/* Number of kernels this context has launched (eager launches plus kernels inside
+ * replayed graphs), for launch accounting. */
+qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

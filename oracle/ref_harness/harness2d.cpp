@@ -92,8 +92,10 @@ class RefHarness2D : public DMHD2D {
     } else if (h.mode == REF_MODE_RUN || h.mode == REF_MODE_DRUN) {
       setdt(1);
       for (int s = 0; s < h.nsteps; s++) {
+        double ts = omp_get_wtime();
         n++;
         one_step(h.flg, h.mode == REF_MODE_DRUN, dts);
+        step_times.push_back(omp_get_wtime() - ts);
         steps++;
       }
     } else if (h.mode == REF_MODE_EXEC) {
@@ -111,6 +113,7 @@ class RefHarness2D : public DMHD2D {
   double time_now() const { return tim; }
   double dt_now() const { return dt; }
   double *const *state() const { return val; }
+  std::vector<double> step_times;
 };
 
 int main(int argc, char **argv)
@@ -143,6 +146,7 @@ int main(int argc, char **argv)
   r.dt = sim->dt_now();
   r.elapsed_s = elapsed;
   ref_write_result(argv[2], r, dts, sim->state(), r.nd);
+  ref_append_times(argv[2], sim->step_times);
   delete sim;
   return 0;
 }

@@ -51,8 +51,10 @@ class RefHarness3D : public MHD3D {
     } else if (h.mode == REF_MODE_RUN) {
       setdt(1);
       for (int s = 0; s < h.nsteps; s++) {
+        double ts = omp_get_wtime();
         n++;
         one_step(h.flg, dts);
+        step_times.push_back(omp_get_wtime() - ts);
         steps++;
       }
     } else if (h.mode == REF_MODE_EXEC) {
@@ -70,6 +72,7 @@ class RefHarness3D : public MHD3D {
   double time_now() const { return tim; }
   double dt_now() const { return dt; }
   double *const *state() const { return val; }
+  std::vector<double> step_times;
   long cells() const { return (long)nd; }
 };
 
@@ -102,6 +105,7 @@ int main(int argc, char **argv)
   r.dt = sim->dt_now();
   r.elapsed_s = elapsed;
   ref_write_result(argv[2], r, dts, sim->state(), r.nd);
+  ref_append_times(argv[2], sim->step_times);
   delete sim;
   return 0;
 }

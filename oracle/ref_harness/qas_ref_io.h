@@ -5,8 +5,8 @@
  * Input  : RefCaseHeader, then 8 arrays (ro,mx,my,mz,bx,by,bz,en) of nd doubles,
  *          each in the reference layout ss = nx*(ny*k+j)+i with 4 ghost cells
  *          per side (2D/SERIAL/OTvortex/mhd2d_class.hpp:10-12).
- * Output : RefResultHeader, n_dt doubles (dt used by each step), then the 8
- *          arrays after the run.
+ * Output : RefResultHeader, n_dt doubles (dt used by each step), the 8 arrays
+ *          after the run, then int32 count + per-step wall times (RUN modes).
  */
 #ifndef QAS_REF_IO_H
 #define QAS_REF_IO_H
@@ -75,6 +75,17 @@ static inline void ref_write_result(const char *path, const RefResultHeader &r,
   fwrite(&r, sizeof(r), 1, f);
   if (!dts.empty()) fwrite(dts.data(), sizeof(double), dts.size(), f);
   for (int m = 0; m < 8; m++) fwrite(val[m], sizeof(double), (size_t)nd, f);
+  fclose(f);
+}
+
+/* Per-step wall times of the RUN modes, appended after the state (count, then values). */
+static inline void ref_append_times(const char *path, const std::vector<double> &t)
+{
+  FILE *f = fopen(path, "ab");
+  if (!f) ref_die("cannot append output");
+  int32_t n = (int32_t)t.size();
+  fwrite(&n, sizeof(n), 1, f);
+  if (n) fwrite(t.data(), sizeof(double), t.size(), f);
   fclose(f);
 }
 

@@ -70,7 +70,13 @@ def read_result(path: str, prob):
     off += 8 * ndt
     st = np.frombuffer(raw, dtype=np.float64, count=8 * nd, offset=off).copy()
     st = st.reshape(8, prob.nz, prob.ny, prob.nx)
-    return {"state": st, "dts": dts, "steps": steps, "tim": tim, "dt": dt, "elapsed": elapsed}
+    off += 8 * 8 * nd
+    step_times = np.zeros(0)
+    if off + 4 <= len(raw):
+        (nt,) = struct.unpack_from("<i", raw, off)
+        step_times = np.frombuffer(raw, dtype=np.float64, count=nt, offset=off + 4).copy()
+    return {"state": st, "dts": dts, "steps": steps, "tim": tim, "dt": dt, "elapsed": elapsed,
+            "step_times": step_times}
 
 
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,

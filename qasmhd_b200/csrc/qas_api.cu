@@ -1,0 +1,840 @@
+// qas_api.cu -- C-ABI of libqas (include/qas.h): contexts, ghost-fill maps,
+// stage sequencing, the device-resident exec_() loop and its CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qas.h"
+#include "qas_dissip.cuh"
+#include "qas_kernels.cuh"
+
+using namespace qas;
+
+namespace {
+
+thread_local std::string g_last_cuda_error;
+
+constexpr int BLK = 128;     // threads per block of the cell kernels
+constexpr int NSUB_CAP = 8;  // device-guarded cap on dissipative sub-cycles per step
+
+qas_status cuda_fail(cudaError_t e, const char *what)
+{
+  g_last_cuda_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? QAS_ERR_NOMEM : QAS_ERR_CUDA;
+}
+
+#define QAS_CUDA(call)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+double hmin(double a, double b) { return (a >= b) ? b : a; }  // common/common_func.h:11-15
+
+}  // namespace
+
+struct qas_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  qas_grid grid{};
+  qas_scheme scheme{};
+  qas_bc bc{};
+  Geo geo{};
+  double dr = 0.0;
+  // device memory
+  void *pool = nullptr;
+  size_t pool_bytes = 0;
+  int *d_src = nullptr;
+  double *d_fac = nullptr;
+  Ctl *d_ctl = nullptr;
+  DCtl *d_dctl = nullptr;
+  unsigned long long *d_scratch = nullptr;
+  Ctl *h_ctl = nullptr;  // pinned mirror
+  View view{};
+  // run state
+  bool run_initialised = false;
+  // graph of two exec_ steps (odd then even n), keyed by its settings
+  cudaGraphExec_t graph = nullptr;
+  int graph_flg = -1, graph_rule = -1;
+  double graph_cfl = 0.0, graph_nu0 = -1.0, graph_eta0 = -1.0, graph_dtrec = 0.0;
+  int graph_nout = 0;
+  long long graph_kernels = 0;
+  long long launches = 0;
+  bool capturing = false;
+  qas_status latched = QAS_OK;
+};
+
+// ---------------------------------------------------------------------------
+// ghost-fill maps: replay the reference's fill passes on (source, factor) pairs
+// ---------------------------------------------------------------------------
+namespace {
+
+struct AxisMap {
+  std::vector<int> src;
+  std::vector<double> fac;
+  explicit AxisMap(int n) : src(n), fac(n, 1.0)
+  {
+    for (int i = 0; i < n; i++) src[i] = i;
+  }
+  void write(int dst, int s, double f)
+  {
+    src[dst] = src[s];
+    fac[dst] = f * fac[s];
+  }
+};
+
+// periodic copies (common/common_func.c:67-74; mpi/common_mpi.c:256-268)
+void pass_periodic(AxisMap &m, int n)
+{
+  for (int i = 0; i < GH; i++) {
+    m.write(n - 1 - i, 2 * GH - 1 - i, 1.0);
+    m.write(i, n - 2 * GH + i, 1.0);
+  }
+}
+
+// Neumann/Dirichlet (|dn|=1) and open/zero-fixed (|dn|=2) passes (common_func.c:75-99)
+void pass_physical(AxisMap &m, int n, int st, int dn)
+{
+  if (dn == 1 || dn == -1) {
+    for (int i = 0; i < GH; i++) m.write(i, 2 * GH - 1 + st - i, (double)dn);
+    for (int i = 0; i < GH - st; i++) m.write(n - 1 - i, n - 2 * GH + st + i, (double)dn);
+  } else if (dn == 2 || dn == -2) {
+    const double c = 0.25 * (2 + dn);
+    for (int i = 0; i < GH; i++) m.write(i, GH, c);
+    for (int i = 0; i < GH - st; i++) m.write(n - 1 - i, n - 1 - GH + st, c);
+  }
+}
+
+bool flag_ok(int dn) { return dn == 0 || dn == 1 || dn == -1 || dn == 2 || dn == -2; }
+
+// Build one axis map.  dim 1/2: the field's own flag decides periodic vs physical
+// (bc1d/bc2d).  dim 3: the group's first flag decides the periodic copy for all its
+// fields, then the field's physical pass (mpi_sdrv3d + mpi_x/y/zbc3d).
+bool build_axis(AxisMap &m, int dim, int n, int st, int dn, int group_dn)
+{
+  if (!flag_ok(dn) || !flag_ok(group_dn)) return false;
+  if (dim <= 2) {
+    if (dn == 0)
+      pass_periodic(m, n);
+    else
+      pass_physical(m, n, dim == 1 ? 0 : st, dn);
+  } else {
+    if (group_dn == 0) pass_periodic(m, n);
+    if (dn != 0) pass_physical(m, n, st, dn);
+    if (dn == 0 && group_dn != 0) return false;  // ghosts left unset by the reference
+  }
+  // every source must be a cell this axis' passes never write
+  for (int i = 0; i < n; i++)
+    if (m.src[m.src[i]] != m.src[i]) return false;
+  return true;
+}
+
+}  // namespace
+
+// One (group, field, axis) map.  Groups: 0 the state (bound(val)), 1 cell-centre B
+// (bound(cx,cy,cz) with bx/by/bz's flags, unstaggered: mhd2d_solve.cpp:75-79), 2 the shock
+// detector dv (normal component's flag sign-flipped: mhd2d_solve.cpp:119-125).
+static bool map_for(int dim, const qas_bc &bc, int G, int f, int a, int n, AxisMap &m)
+{
+  if (a >= dim) return true;
+  const int *dn[3] = {bc.dnx, bc.dny, bc.dnz};
+  const int st_state[3][8] = {{0, 0, 0, 0, 1, 0, 0, 0}, {0, 0, 0, 0, 0, 1, 0, 0}, {0, 0, 0, 0, 0, 0, 1, 0}};
+  int fdn, gdn, st;
+  if (G == 0) {
+    fdn = dn[a][f];
+    gdn = dn[a][0];
+    st = st_state[a][f];
+  } else if (G == 1) {
+    fdn = dn[a][4 + f];
+    gdn = dn[a][4];
+    st = 0;
+  } else {
+    auto dvflag = [&](int comp) { return comp == a ? -dn[a][1 + comp] : dn[a][1 + comp]; };
+    fdn = dvflag(f);
+    gdn = dvflag(0);
+    st = 0;
+  }
+  return build_axis(m, dim, n, st, fdn, gdn);
+}
+
+static qas_status build_maps(qas_ctx *c)
+{
+  const int dim = c->grid.dim;
+  const int nmax = std::max(c->geo.nx, std::max(c->geo.ny, c->geo.nz));
+  std::vector<int> src((size_t)3 * 8 * 3 * nmax, 0);
+  std::vector<double> fac((size_t)3 * 8 * 3 * nmax, 1.0);
+  for (int G = 0; G < 3; G++) {
+    const int nf = G == 0 ? 8 : 3;
+    for (int f = 0; f < nf; f++) {
+      for (int a = 0; a < 3; a++) {
+        const int n = c->geo.n[a];
+        AxisMap m(n);
+        if (!map_for(dim, c->bc, G, f, a, n, m)) return QAS_ERR_INVALID;
+        const size_t base = (size_t)((G * 8 + f) * 3 + a) * nmax;
+        for (int i = 0; i < n; i++) {
+          src[base + i] = m.src[i];
+          fac[base + i] = m.fac[i];
+        }
+      }
+    }
+  }
+  QAS_CUDA(cudaMalloc(&c->d_src, src.size() * sizeof(int)));
+  QAS_CUDA(cudaMalloc(&c->d_fac, fac.size() * sizeof(double)));
+  QAS_CUDA(cudaMemcpy(c->d_src, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice));
+  QAS_CUDA(cudaMemcpy(c->d_fac, fac.data(), fac.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c->view.maps.src = c->d_src;
+  c->view.maps.fac = c->d_fac;
+  c->view.maps.nmax = nmax;
+  return QAS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+namespace {
+
+dim3 cells_grid(const Geo &g) { return dim3((g.nx + BLK - 1) / BLK, g.ny, g.nz); }
+dim3 update_grid(const Geo &g)
+{
+  return dim3((g.nx - 2 * GH + 1 + BLK - 1) / BLK, g.dim >= 2 ? g.ny - 2 * GH + 1 : 1,
+              g.dim >= 3 ? g.nz - 2 * GH + 1 : 1);
+}
+dim3 interior_grid(const Geo &g)
+{
+  return dim3((g.nx - 2 * GH + BLK - 1) / BLK, g.dim >= 2 ? g.ny - 2 * GH : 1, g.dim >= 3 ? g.nz - 2 * GH : 1);
+}
+
+template <int ODR>
+void launch_lr(qas_ctx *c, int a)
+{
+  const dim3 gr = cells_grid(c->geo);
+  if (a == 0) k_lr<ODR, 0><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 1) k_lr<ODR, 1><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 2) k_lr<ODR, 2><<<gr, BLK, 0, c->stream>>>(c->view);
+}
+template <int RMN>
+void launch_flux(qas_ctx *c, int a)
+{
+  const dim3 gr = cells_grid(c->geo);
+  if (a == 0) k_flux<RMN, 0><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 1) k_flux<RMN, 1><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 2) k_flux<RMN, 2><<<gr, BLK, 0, c->stream>>>(c->view);
+}
+
+template <int ODR>
+long long stage_odr(qas_ctx *c, double c0, double c1)
+{
+  const Geo &g = c->geo;
+  long long nk = 0;
+  k_prim<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+  nk++;
+  if (c->scheme.rmn >= 2 && g.dim >= 2) {
+    k_dv<<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+    nk++;
+  }
+  for (int a = 0; a < g.dim; a++) {
+    launch_lr<ODR>(c, a);
+    switch (c->scheme.rmn) {
+      case 0: launch_flux<0>(c, a); break;
+      case 1: launch_flux<1>(c, a); break;
+      case 2: launch_flux<2>(c, a); break;
+      default: launch_flux<3>(c, a); break;
+    }
+    nk += 2;
+  }
+  if (g.dim >= 2) {
+    k_emf<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+    nk++;
+  }
+  k_update<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c0, c1);
+  k_bound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+  nk += 2;
+  return nk;
+}
+
+// rk_fac table of mhd2d_solve.cpp:7 for the context's R_K
+void rk_factors(int R_K, int rk, double &c0, double &c1)
+{
+  const double t[3][2] = {{0.0, 1.0}, {0.5 + (R_K - 2) * 0.25, 0.5 - (R_K - 2) * 0.25}, {1. / 3., 2. / 3.}};
+  c0 = t[rk][0];
+  c1 = t[rk][1];
+}
+
+// ideal(dt) on the device, dt and dt/dx already in the control block
+long long launch_ideal(qas_ctx *c)
+{
+  long long nk = 0;
+  const size_t bytes = (size_t)c->geo.nd * sizeof(double);
+  for (int m = 0; m < 8; m++) cudaMemcpyAsync(c->view.u0[m], c->view.u[m], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  for (int rk = 0; rk < c->scheme.rk; rk++) {
+    double c0, c1;
+    rk_factors(c->scheme.rk, rk, c0, c1);
+    switch (c->scheme.odr) {
+      case 1: nk += stage_odr<1>(c, c0, c1); break;
+      case 2: nk += stage_odr<2>(c, c0, c1); break;
+      case 3: nk += stage_odr<3>(c, c0, c1); break;
+      default: nk += stage_odr<4>(c, c0, c1); break;
+    }
+  }
+  return nk;
+}
+
+template <int ODR>
+long long dsptv_odr(qas_ctx *c, int nc, double nu0, double eta0)
+{
+  const Geo &g = c->geo;
+  const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
+  long long nk = 0;
+  k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
+  k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, nc);
+  nk += 2;
+  for (int rk = 0; rk < c->scheme.rk; rk++) {
+    double c0, c1;
+    rk_factors(c->scheme.rk, rk, c0, c1);
+    k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
+    k_eres<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, eta0, idx, idy);
+    k_dflux<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, nu0, idx, idy);
+    k_dupdate<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, c0, c1);
+    k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
+    nk += 5;
+  }
+  return nk;
+}
+
+long long launch_dsptv(qas_ctx *c, int nc, double nu0, double eta0)
+{
+  switch (c->scheme.odr) {
+    case 1: return dsptv_odr<1>(c, nc, nu0, eta0);
+    case 2: return dsptv_odr<2>(c, nc, nu0, eta0);
+    case 3: return dsptv_odr<3>(c, nc, nu0, eta0);
+    default: return dsptv_odr<4>(c, nc, nu0, eta0);
+  }
+}
+
+// setdc + sub-cycled dsptv after ideal (dmhd2d_class.cpp:19-26), device-guarded
+long long launch_dissipate(qas_ctx *c, double nu0, double eta0)
+{
+  const double dcmax0 = (2 * nu0 >= eta0) ? 2 * nu0 : eta0;
+  const double dcmax = dcmax0 > 0.0 ? dcmax0 : 0.0;
+  if (!(dcmax > 1e-15)) return 0;
+  k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx, 1.0 / c->grid.dy,
+                                       NSUB_CAP);
+  long long nk = 1;
+  for (int nc = 0; nc < NSUB_CAP; nc++) nk += launch_dsptv(c, nc, nu0, eta0);
+  return nk;
+}
+
+long long launch_setdt(qas_ctx *c, double cfl, int rule, double dtrec, int nout)
+{
+  k_vmax_reset<<<1, 1, 0, c->stream>>>(c->view);
+  k_vmax<<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  k_setdt<<<1, 1, 0, c->stream>>>(c->view, cfl, c->dr, rule, dtrec, nout);
+  return 3;
+}
+
+// one exec_ iteration
+long long launch_exec_step(qas_ctx *c, const qas_run_opts &o, int n_after)
+{
+  long long nk = 0;
+  k_begin_step<<<1, 1, 0, c->stream>>>(c->view, o.stop_rule == 2 ? 0 : 1);
+  k_bound<<<cells_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  nk += 2 + launch_ideal(c);
+  if (c->grid.dim == 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
+  if (o.flg && (n_after % 2 == 0)) nk += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
+  return nk;
+}
+
+qas_status check_launch(qas_ctx *c)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return QAS_OK;
+}
+
+qas_status read_ctl(qas_ctx *c)
+{
+  QAS_CUDA(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->h_ctl->err & 4) return QAS_ERR_UNSUPPORTED;
+  if (c->h_ctl->err & 1) return QAS_ERR_NONFINITE;
+  return QAS_OK;
+}
+
+qas_status write_ctl(qas_ctx *c)
+{
+  QAS_CUDA(cudaMemcpyAsync(c->d_ctl, c->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  return QAS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *qas_status_str(qas_status s)
+{
+  switch (s) {
+    case QAS_OK: return "ok";
+    case QAS_ERR_INVALID: return "invalid argument";
+    case QAS_ERR_CUDA: return "CUDA error";
+    case QAS_ERR_NOMEM: return "out of device memory";
+    case QAS_ERR_NONFINITE: return "non-finite or non-positive state detected on the device";
+    case QAS_ERR_TIMEOUT: return "bounded device wait timed out";
+    case QAS_ERR_UNSUPPORTED: return "unsupported configuration";
+    case QAS_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+int qas_abi_version(void) { return QAS_ABI_VERSION; }
+
+const char *qas_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *scheme, const qas_bc *bc, int device)
+{
+  if (!out || !grid || !scheme || !bc) return QAS_ERR_INVALID;
+  *out = nullptr;
+  const qas_grid &gr = *grid;
+  if (gr.dim < 1 || gr.dim > 3 || gr.nxm < 4) return QAS_ERR_INVALID;
+  if (gr.dim >= 2 && gr.nym < 4) return QAS_ERR_INVALID;
+  if (gr.dim >= 3 && gr.nzm < 4) return QAS_ERR_INVALID;
+  if (!(gr.dx > 0) || (gr.dim >= 2 && !(gr.dy > 0)) || (gr.dim >= 3 && !(gr.dz > 0))) return QAS_ERR_INVALID;
+  if (scheme->rmn < 0 || scheme->rmn > 3 || scheme->odr < 1 || scheme->odr > 4 || scheme->rk < 1 ||
+      scheme->rk > 3)
+    return QAS_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return QAS_ERR_NO_DEVICE;
+  qas_ctx *c = new (std::nothrow) qas_ctx();
+  if (!c) return QAS_ERR_NOMEM;
+  c->grid = gr;
+  c->scheme = *scheme;
+  c->bc = *bc;
+  if (device >= 0) {
+    if (cudaSetDevice(device) != cudaSuccess) {
+      delete c;
+      return QAS_ERR_NO_DEVICE;
+    }
+    c->device = device;
+  } else {
+    cudaGetDevice(&c->device);
+  }
+  Geo &g = c->geo;
+  g.dim = gr.dim;
+  g.nx = gr.nxm + 2 * GH;
+  g.ny = gr.dim >= 2 ? gr.nym + 2 * GH : 1;
+  g.nz = gr.dim >= 3 ? gr.nzm + 2 * GH : 1;
+  g.nd = (long long)g.nx * g.ny * g.nz;
+  g.s[0] = 1;
+  g.s[1] = g.nx;
+  g.s[2] = (long long)g.nx * g.ny;
+  g.n[0] = g.nx;
+  g.n[1] = g.ny;
+  g.n[2] = g.nz;
+  c->dr = gr.dim == 1 ? gr.dx : (gr.dim == 2 ? hmin(gr.dx, gr.dy) : hmin(hmin(gr.dx, gr.dy), gr.dz));
+
+  qas_status st = QAS_OK;
+  auto fail = [&](qas_status s) {
+    qas_destroy(c);
+    return s;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(QAS_ERR_CUDA);
+  if ((st = build_maps(c)) != QAS_OK) return fail(st);
+
+  // one pool for every field array, 256-byte aligned
+  const size_t arr = ((size_t)g.nd * sizeof(double) + 255) & ~(size_t)255;
+  const int n_arrays = 8 + 8 + 7 + 3 + 14 + 4 + 24 + 6 + 3;
+  c->pool_bytes = arr * n_arrays;
+  if (cudaMalloc(&c->pool, c->pool_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(QAS_ERR_NOMEM);
+  }
+  if (cudaMemsetAsync(c->pool, 0, c->pool_bytes, c->stream) != cudaSuccess) return fail(QAS_ERR_CUDA);
+  char *p = (char *)c->pool;
+  auto take = [&]() {
+    double *r = (double *)p;
+    p += arr;
+    return r;
+  };
+  View &v = c->view;
+  v.g = g;
+  v.rmn = scheme->rmn;
+  v.odr = scheme->odr;
+  v.rk = scheme->rk;
+  v.ctw = scheme->ctw ? 1 : 0;
+  v.gam = gr.gam;
+  v.dx = gr.dx;
+  v.dy = gr.dim >= 2 ? gr.dy : 1.0;
+  v.dz = gr.dim >= 3 ? gr.dz : 1.0;
+  for (int m = 0; m < 8; m++) v.u[m] = take();
+  for (int m = 0; m < 8; m++) v.u0[m] = take();
+  v.vx = take(); v.vy = take(); v.vz = take(); v.pr = take();
+  v.cx = take(); v.cy = take(); v.cz = take();
+  for (int a = 0; a < 3; a++) v.dv[a] = take();
+  for (int m = 0; m < 7; m++) v.vl[m] = take();
+  for (int m = 0; m < 7; m++) v.vr[m] = take();
+  for (int t = 0; t < 2; t++) v.ql[t] = take();
+  for (int t = 0; t < 2; t++) v.qr[t] = take();
+  for (int a = 0; a < 3; a++)
+    for (int m = 0; m < 8; m++) v.f[a][m] = take();
+  for (int a = 0; a < 3; a++)
+    for (int t = 0; t < 2; t++) v.fc[a][t] = take();
+  v.ex = take(); v.ey = take(); v.ez = take();
+
+  if (cudaMalloc(&c->d_ctl, sizeof(Ctl)) != cudaSuccess) return fail(QAS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_dctl, sizeof(DCtl)) != cudaSuccess) return fail(QAS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_scratch, 64) != cudaSuccess) return fail(QAS_ERR_NOMEM);
+  if (cudaMallocHost(&c->h_ctl, sizeof(Ctl)) != cudaSuccess) return fail(QAS_ERR_NOMEM);
+  memset(c->h_ctl, 0, sizeof(Ctl));
+  c->h_ctl->nmax = INT_MAX;
+  c->h_ctl->tmax = INFINITY;
+  c->h_ctl->first = 1;
+  v.ctl = c->d_ctl;
+  if (cudaMemsetAsync(c->d_dctl, 0, sizeof(DCtl), c->stream) != cudaSuccess) return fail(QAS_ERR_CUDA);
+  if ((st = write_ctl(c)) != QAS_OK) return fail(st);
+  *out = c;
+  return QAS_OK;
+}
+
+qas_status qas_destroy(qas_ctx *c)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->pool) cudaFree(c->pool);
+  if (c->d_src) cudaFree(c->d_src);
+  if (c->d_fac) cudaFree(c->d_fac);
+  if (c->d_ctl) cudaFree(c->d_ctl);
+  if (c->d_dctl) cudaFree(c->d_dctl);
+  if (c->d_scratch) cudaFree(c->d_scratch);
+  if (c->h_ctl) cudaFreeHost(c->h_ctl);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return QAS_OK;
+}
+
+qas_status qas_cells(const qas_ctx *c, long long *nd)
+{
+  if (!c || !nd) return QAS_ERR_INVALID;
+  *nd = c->geo.nd;
+  return QAS_OK;
+}
+
+qas_status qas_upload(qas_ctx *c, double *const val[8])
+{
+  if (!c || !val) return QAS_ERR_INVALID;
+  const size_t bytes = (size_t)c->geo.nd * sizeof(double);
+  for (int m = 0; m < 8; m++) {
+    if (!val[m]) return QAS_ERR_INVALID;
+    QAS_CUDA(cudaMemcpyAsync(c->view.u[m], val[m], bytes, cudaMemcpyHostToDevice, c->stream));
+  }
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  return QAS_OK;
+}
+
+qas_status qas_download(qas_ctx *c, double *val[8])
+{
+  if (!c || !val) return QAS_ERR_INVALID;
+  const size_t bytes = (size_t)c->geo.nd * sizeof(double);
+  for (int m = 0; m < 8; m++) {
+    if (!val[m]) return QAS_ERR_INVALID;
+    QAS_CUDA(cudaMemcpyAsync(val[m], c->view.u[m], bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  return QAS_OK;
+}
+
+qas_status qas_upload_block(qas_ctx *c, const double *block)
+{
+  if (!c || !block) return QAS_ERR_INVALID;
+  double *val[8];
+  for (int m = 0; m < 8; m++) val[m] = (double *)block + (size_t)m * c->geo.nd;
+  return qas_upload(c, val);
+}
+
+qas_status qas_download_block(qas_ctx *c, double *block)
+{
+  if (!c || !block) return QAS_ERR_INVALID;
+  double *val[8];
+  for (int m = 0; m < 8; m++) val[m] = block + (size_t)m * c->geo.nd;
+  return qas_download(c, val);
+}
+
+qas_status qas_device_state(qas_ctx *c, double **d_block)
+{
+  if (!c || !d_block) return QAS_ERR_INVALID;
+  // the state arrays are consecutive in the pool with a 256-byte aligned stride; callers
+  // that need a dense block use qas_upload_block / qas_download_block
+  *d_block = c->view.u[0];
+  return QAS_OK;
+}
+
+qas_status qas_stream(qas_ctx *c, void **stream)
+{
+  if (!c || !stream) return QAS_ERR_INVALID;
+  *stream = (void *)c->stream;
+  return QAS_OK;
+}
+
+qas_status qas_bound(qas_ctx *c)
+{
+  if (!c) return QAS_ERR_INVALID;
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  k_bound<<<cells_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  c->launches++;
+  return check_launch(c);
+}
+
+qas_status qas_step(qas_ctx *c, double dt)
+{
+  if (!c) return QAS_ERR_INVALID;
+  // a single ideal(dt): make sure the loop's done flag does not mask the kernels
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
+  c->launches += 1 + launch_ideal(c);
+  return check_launch(c);
+}
+
+qas_status qas_cfl_vmax(qas_ctx *c, double *vmax)
+{
+  if (!c || !vmax) return QAS_ERR_INVALID;
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  k_vmax_reset<<<1, 1, 0, c->stream>>>(c->view);
+  k_vmax<<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  c->launches += 2;
+  qas_status s = check_launch(c);
+  if (s != QAS_OK) return s;
+  QAS_CUDA(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  unsigned long long b = c->h_ctl->vmax_bits;
+  memcpy(vmax, &b, sizeof(double));
+  return QAS_OK;
+}
+
+qas_status qas_cfl_dt(qas_ctx *c, double cfl, double *dt)
+{
+  if (!dt) return QAS_ERR_INVALID;
+  double vmax = 0.0;
+  qas_status s = qas_cfl_vmax(c, &vmax);
+  if (s != QAS_OK) return s;
+  *dt = cfl * c->dr / vmax;
+  return QAS_OK;
+}
+
+qas_status qas_run_reset(qas_ctx *c)
+{
+  if (!c) return QAS_ERR_INVALID;
+  c->run_initialised = false;
+  return QAS_OK;
+}
+
+qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
+{
+  if (!c || !opts) return QAS_ERR_INVALID;
+  qas_run_opts o = *opts;
+  if (o.stop_rule < 0 || o.stop_rule > 2) return QAS_ERR_INVALID;
+  if (o.stop_rule == 0 && o.max_steps <= 0) return QAS_ERR_INVALID;
+  if ((o.nu0 > 0.0 || o.eta0 > 0.0) && c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  qas_status s;
+  if (!c->run_initialised) {
+    // setdt(1) of main(): dt and nmax from the initial state
+    memset(c->h_ctl, 0, sizeof(Ctl));
+    c->h_ctl->first = 1;
+    c->h_ctl->nmax = INT_MAX;
+    c->h_ctl->tmax = o.stop_rule == 0 ? INFINITY : o.dtrec * o.nout;
+    if ((s = write_ctl(c)) != QAS_OK) return s;
+    c->launches += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
+    if ((s = check_launch(c)) != QAS_OK) return s;
+    c->run_initialised = true;
+  } else {
+    if ((s = read_ctl(c)) != QAS_OK) return s;
+    c->h_ctl->done = 0;
+    if (o.stop_rule == 0) c->h_ctl->nmax = INT_MAX;
+    if ((s = write_ctl(c)) != QAS_OK) return s;
+  }
+  if ((s = read_ctl(c)) != QAS_OK) return s;
+  const int n0 = c->h_ctl->n;
+  int n_host = n0;
+  const int limit = o.max_steps > 0 ? o.max_steps : INT_MAX;
+  int launched = 0;
+  // odd n: one eager step so graphs always start at an even n
+  if (n_host % 2 == 1 && launched < limit) {
+    c->launches += launch_exec_step(c, o, n_host + 1);
+    n_host++;
+    launched++;
+  }
+  const bool want_graph = o.use_graph != 0;
+  if (want_graph && launched + 2 <= limit) {
+    const bool stale = !c->graph || c->graph_flg != o.flg || c->graph_rule != o.stop_rule || c->graph_cfl != o.cfl ||
+                       c->graph_nu0 != o.nu0 || c->graph_eta0 != o.eta0 || c->graph_dtrec != o.dtrec ||
+                       c->graph_nout != o.nout;
+    if (stale) {
+      if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+      }
+      cudaGraph_t gph;
+      QAS_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      long long nk = launch_exec_step(c, o, 1) + launch_exec_step(c, o, 2);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &gph);
+      if (e != cudaSuccess) return cuda_fail(e, "graph capture");
+      e = cudaGraphInstantiate(&c->graph, gph, 0);
+      cudaGraphDestroy(gph);
+      if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+      c->graph_kernels = nk;
+      c->graph_flg = o.flg;
+      c->graph_rule = o.stop_rule;
+      c->graph_cfl = o.cfl;
+      c->graph_nu0 = o.nu0;
+      c->graph_eta0 = o.eta0;
+      c->graph_dtrec = o.dtrec;
+      c->graph_nout = o.nout;
+    }
+  }
+  const int chunk = 32;  // steps between host checks of the stop flag
+  while (launched < limit) {
+    int this_chunk = 0;
+    while (this_chunk < chunk && launched < limit) {
+      if (want_graph && c->graph && launched + 2 <= limit) {
+        QAS_CUDA(cudaGraphLaunch(c->graph, c->stream));
+        c->launches += c->graph_kernels;
+        launched += 2;
+        n_host += 2;
+        this_chunk += 2;
+      } else {
+        c->launches += launch_exec_step(c, o, n_host + 1);
+        launched++;
+        n_host++;
+        this_chunk++;
+      }
+    }
+    if ((s = check_launch(c)) != QAS_OK) return s;
+    if (o.stop_rule != 0) {
+      if ((s = read_ctl(c)) != QAS_OK) return s;
+      if (c->h_ctl->done) break;
+    }
+  }
+  if ((s = read_ctl(c)) != QAS_OK) return s;
+  if (info) {
+    info->steps = c->h_ctl->n - n0;
+    info->n = c->h_ctl->n;
+    info->nmax = c->h_ctl->nmax;
+    info->tim = c->h_ctl->tim;
+    info->dt = c->h_ctl->dt;
+  }
+  return QAS_OK;
+}
+
+qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  k_dsub_fixed<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dt, 1.0 / c->grid.dx, 1.0 / c->grid.dy);
+  // dsptv itself does not fill the ghosts first; launch_dsptv starts with a fill, so
+  // run the body without it: copy, stages
+  const Geo &g = c->geo;
+  const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
+  k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, 0);
+  long long nk = 2;
+  for (int rk = 0; rk < c->scheme.rk; rk++) {
+    double c0, c1;
+    rk_factors(c->scheme.rk, rk, c0, c1);
+    switch (c->scheme.odr) {
+#define QAS_DST(O)                                                                                        \
+  case O:                                                                                                 \
+    k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                  \
+    k_eres<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, eta0, idx, idy);               \
+    k_dflux<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, nu0, idx, idy);               \
+    k_dupdate<O><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, c0, c1);                   \
+    k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                \
+    break;
+      QAS_DST(1)
+      QAS_DST(2)
+      QAS_DST(3)
+      default:
+      QAS_DST(4)
+#undef QAS_DST
+    }
+    nk += 5;
+  }
+  c->launches += nk;
+  return check_launch(c);
+}
+
+qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
+  c->launches += 1 + launch_dissipate(c, nu0, eta0);
+  return check_launch(c);
+}
+
+qas_status qas_max_divb(qas_ctx *c, double *maxdivb)
+{
+  if (!c || !maxdivb) return QAS_ERR_INVALID;
+  if (c->grid.dim < 2) {
+    *maxdivb = 0.0;
+    return QAS_OK;
+  }
+  QAS_CUDA(cudaMemsetAsync(c->d_scratch, 0, sizeof(unsigned long long), c->stream));
+  switch (c->scheme.odr) {
+    case 1: k_divb<1><<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view, c->d_scratch); break;
+    case 2: k_divb<2><<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view, c->d_scratch); break;
+    case 3: k_divb<3><<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view, c->d_scratch); break;
+    default: k_divb<4><<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view, c->d_scratch); break;
+  }
+  c->launches++;
+  qas_status s = check_launch(c);
+  if (s != QAS_OK) return s;
+  unsigned long long bits = 0;
+  QAS_CUDA(cudaMemcpyAsync(&bits, c->d_scratch, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  memcpy(maxdivb, &bits, sizeof(double));
+  return QAS_OK;
+}
+
+qas_status qas_sync(qas_ctx *c)
+{
+  if (!c) return QAS_ERR_INVALID;
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  return read_ctl(c);
+}
+
+qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int field, int axis, int *src,
+                      double *fac, int n)
+{
+  if (!grid || !bc || !src || !fac) return QAS_ERR_INVALID;
+  if (group < 0 || group > 2 || field < 0 || field >= (group == 0 ? 8 : 3) || axis < 0 || axis > 2)
+    return QAS_ERR_INVALID;
+  const int ext[3] = {grid->nxm + 2 * GH, grid->dim >= 2 ? grid->nym + 2 * GH : 1,
+                      grid->dim >= 3 ? grid->nzm + 2 * GH : 1};
+  if (n != ext[axis]) return QAS_ERR_INVALID;
+  AxisMap m(n);
+  if (!map_for(grid->dim, *bc, group, field, axis, n, m)) return QAS_ERR_INVALID;
+  for (int i = 0; i < n; i++) {
+    src[i] = m.src[i];
+    fac[i] = m.fac[i];
+  }
+  return QAS_OK;
+}
+
+qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
+{
+  if (!c || !count) return QAS_ERR_INVALID;
+  *count = c->launches;
+  return QAS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+// qas_dissip.cuh -- visco-resistive update of the 2D driver on sm_100a:
+// DMHD2D::dsptv (2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151) with uniform nu, eta,
+// sub-cycled as in DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26).
+#pragma once
+
+#include "qas_kernels.cuh"
+
+namespace qas {
+
+// Extra device control for the sub-cycles: ncmax and dt/ncmax of the current step.
+struct DCtl {
+  int ncmax;
+  int pad;
+  double sdt;      // dt/ncmax
+  double sdtd[2];  // sdt*idx, sdt*idy
+};
+
+// setdc + ncmax = 1 + (int)(2*(dcmax*dt)/(dr*dr))
+__global__ void k_dsub_setup(View v, DCtl *dc, double dcmax, double dr, double idx, double idy, int cap)
+{
+  if (v.ctl->done) return;
+  const double dt = v.ctl->dt;
+  int ncmax = 0;
+  if (dcmax > 1e-15) ncmax = 1 + (int)(2 * (dcmax * dt) / (dr * dr));
+  if (ncmax > cap) {
+    atomicOr(&v.ctl->err, 4);
+    ncmax = cap;
+  }
+  dc->ncmax = ncmax;
+  dc->sdt = ncmax > 0 ? dt / ncmax : 0.0;
+  dc->sdtd[0] = dc->sdt * idx;
+  dc->sdtd[1] = dc->sdt * idy;
+}
+
+// host-supplied dt for one dsptv(dt) call
+__global__ void k_dsub_fixed(View v, DCtl *dc, double dt, double idx, double idy)
+{
+  dc->ncmax = 1;
+  dc->sdt = dt;
+  dc->sdtd[0] = dt * idx;
+  dc->sdtd[1] = dt * idy;
+}
+
+#define QAS_DSUB_GUARD()                        \
+  if (v.ctl->done || nc >= dc->ncmax) return;
+
+// velocity at every cell (vlcty, common/mhd_class.hpp:59-65)
+__global__ void k_dvel(View v, const DCtl *dc, int nc)
+{
+  QAS_DSUB_GUARD();
+  QAS_CELL_INDEX();
+  const long long c = cidx(v.g, i, j, k);
+  const double iro = 1.0 / v.u[0][c];
+  v.vx[c] = v.u[1][c] * iro;
+  v.vy[c] = v.u[2][c] * iro;
+  v.vz[c] = v.u[3][c] * iro;
+}
+
+// eta*J on the CT edges, mhd_ct_eres (common/mhd_func.c:78-106) with zoffset=0, idz=0
+template <int ODR>
+__global__ void k_eres(View v, const DCtl *dc, int nc, double eta0, double idx, double idy)
+{
+  QAS_DSUB_GUARD();
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  if (i < 2 || i >= g.nx - 1 || j < 2 || j >= g.ny - 1) return;
+  const long long c = cidx(g, i, j, k);
+  const long long sy = g.s[1];
+  const double *bx = v.u[4], *by = v.u[5], *bz = v.u[6];
+  const double idz = 0.0;
+  // derivatives along the absent z axis see four equal values
+  const double dbxz = dfc<ODR>(bx[c], bx[c], bx[c], bx[c]);
+  const double dbyz = dfc<ODR>(by[c], by[c], by[c], by[c]);
+  const double jx = dfc<ODR>(bz[c - 2 * sy], bz[c - sy], bz[c], bz[c + sy]) * idy - dbyz * idz;
+  const double jy = dbxz * idz - dfc<ODR>(bz[c - 2], bz[c - 1], bz[c], bz[c + 1]) * idx;
+  const double jz = dfc<ODR>(by[c - 2], by[c - 1], by[c], by[c + 1]) * idx -
+                    dfc<ODR>(bx[c - 2 * sy], bx[c - sy], bx[c], bx[c + sy]) * idy;
+  const double e = eta0;
+  v.ex[c] = 0.25 * (e + e + e + e) * jx;
+  v.ey[c] = 0.25 * (e + e + e + e) * jy;
+  v.ez[c] = 0.25 * (e + e + e + e) * jz;
+}
+
+// viscous face flux at i-1/2 along stride xo with transverse strides yo, zo (0 for the
+// absent axis), calc_flux_viscous (common/mhd_flux.c:700-752); returns fmx, fmy, fmz, fen.
+template <int ODR>
+__device__ __forceinline__ void visc_flux(const double *vx, const double *vy, const double *vz, long long c,
+                                          double rnu, double idx, double idy, double idz, long long xo, long long yo,
+                                          long long zo, double &fmx, double &fmy, double &fmz, double &fen)
+{
+  const double c2 = 2. / 3., c4 = 4. / 3.;
+  double a[4], b[4], d[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    a[m] = vx[c + (m - 2) * xo];
+    b[m] = vy[c + (m - 2) * xo];
+    d[m] = vz[c + (m - 2) * xo];
+  }
+  const double vx0 = fcen<ODR>(a[0], a[1], a[2], a[3]);
+  const double vy0 = fcen<ODR>(b[0], b[1], b[2], b[3]);
+  const double vz0 = fcen<ODR>(d[0], d[1], d[2], d[3]);
+  const double dvxdx = dfc<ODR>(a[0], a[1], a[2], a[3]) * idx;
+  const double dvydx = dfc<ODR>(b[0], b[1], b[2], b[3]) * idx;
+  const double dvzdx = dfc<ODR>(d[0], d[1], d[2], d[3]) * idx;
+  double t[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) t[m] = 0.5 * (vx[c + (m - 2) * xo + yo] - vx[c + (m - 2) * xo - yo]);
+  const double dvxdy = fcen<ODR>(t[0], t[1], t[2], t[3]) * idy;
+#pragma unroll
+  for (int m = 0; m < 4; m++) t[m] = 0.5 * (vy[c + (m - 2) * xo + yo] - vy[c + (m - 2) * xo - yo]);
+  const double dvydy = fcen<ODR>(t[0], t[1], t[2], t[3]) * idy;
+#pragma unroll
+  for (int m = 0; m < 4; m++) t[m] = 0.5 * (vx[c + (m - 2) * xo + zo] - vx[c + (m - 2) * xo - zo]);
+  const double dvxdz = fcen<ODR>(t[0], t[1], t[2], t[3]) * idz;
+#pragma unroll
+  for (int m = 0; m < 4; m++) t[m] = 0.5 * (vz[c + (m - 2) * xo + zo] - vz[c + (m - 2) * xo - zo]);
+  const double dvzdz = fcen<ODR>(t[0], t[1], t[2], t[3]) * idz;
+  fmx = -rnu * (c4 * dvxdx - c2 * (dvydy + dvzdz));
+  fmy = -rnu * (dvydx + dvxdy);
+  fmz = -rnu * (dvzdx + dvxdz);
+  fen = fmx * vx0 + fmy * vy0 + fmz * vz0;
+}
+
+// resistive face flux, calc_flux_resistive (common/mhd_flux.c:754-782): B pair (by,bz) with
+// offsets yo (of by) and zo (of bz), E pair (ey averaged over zo, ez over yo).
+template <int ODR>
+__device__ __forceinline__ void resist_flux(const double *by, const double *bz, const double *ey, const double *ez,
+                                            long long c, long long xo, long long yo, long long zo, double &fby,
+                                            double &fbz, double &fen)
+{
+  const double ey0 = 0.5 * (ey[c] + ey[c + zo]);
+  const double ez0 = 0.5 * (ez[c] + ez[c + yo]);
+  double byi[4], bzi[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const long long p = c + (m - 2) * xo;
+    byi[m] = 0.5 * (by[p] + by[p + yo]);
+    bzi[m] = 0.5 * (bz[p] + bz[p + zo]);
+  }
+  const double by0 = fcen<ODR>(byi[0], byi[1], byi[2], byi[3]);
+  const double bz0 = fcen<ODR>(bzi[0], bzi[1], bzi[2], bzi[3]);
+  fby = -ez0;
+  fbz = +ey0;
+  fen = ey0 * bz0 - ez0 * by0;
+}
+
+template <int ODR>
+__global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, double idy)
+{
+  QAS_DSUB_GUARD();
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  if (i < 2 || i >= g.nx - 1 || j < 2 || j >= g.ny - 1) return;
+  const long long c = cidx(g, i, j, k);
+  const long long sy = g.s[1];
+  const double *ro = v.u[0];
+  double fmx, fmy, fmz, fenv, fby, fbz, fenr;
+  // x face (dmhd2d_solve.cpp:70-82)
+  double rnu = 0.5 * (ro[c - 1] * nu0 + ro[c] * nu0);
+  visc_flux<ODR>(v.vx, v.vy, v.vz, c, rnu, idx, idy, 0.0, 1, sy, 0, fmx, fmy, fmz, fenv);
+  resist_flux<ODR>(v.u[5], v.u[6], v.ey, v.ez, c, 1, sy, 0, fby, fbz, fenr);
+  v.f[0][0][c] = 0.0 + 0.0;
+  v.f[0][1][c] = fmx + 0.0;
+  v.f[0][2][c] = fmy + 0.0;
+  v.f[0][3][c] = fmz + 0.0;
+  v.f[0][5][c] = 0.0 + fby;
+  v.f[0][6][c] = 0.0 + fbz;
+  v.f[0][7][c] = fenv + fenr;
+  // y face (dmhd2d_solve.cpp:83-94)
+  rnu = 0.5 * (ro[c - sy] * nu0 + ro[c] * nu0);
+  visc_flux<ODR>(v.vy, v.vz, v.vx, c, rnu, idy, 0.0, idx, sy, 0, 1, fmx, fmy, fmz, fenv);
+  resist_flux<ODR>(v.u[6], v.u[4], v.ez, v.ex, c, sy, 0, 1, fby, fbz, fenr);
+  v.f[1][0][c] = 0.0 + 0.0;
+  v.f[1][2][c] = fmx + 0.0;
+  v.f[1][3][c] = fmy + 0.0;
+  v.f[1][1][c] = fmz + 0.0;
+  v.f[1][6][c] = 0.0 + fby;
+  v.f[1][4][c] = 0.0 + fbz;
+  v.f[1][7][c] = fenv + fenr;
+}
+
+template <int ODR>
+__global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
+{
+  QAS_DSUB_GUARD();
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = GH + blockIdx.y;
+  if (i > g.nx - GH) return;
+  const long long c = cidx(g, i, j, 0);
+  const long long sy = g.s[1];
+  const double dtdx = dc->sdtd[0], dtdy = dc->sdtd[1];
+  const bool ci = i < g.nx - GH, cj = j < g.ny - GH;
+  if (ci && cj) {
+    const int cen[6] = {0, 1, 2, 3, 6, 7};
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int m = cen[q];
+      const double du0 = d4<ODR>(v.f[0][m], c, 1);
+      const double du1 = d4<ODR>(v.f[1][m], c, sy);
+      v.u[m][c] = rk_combine(v.u[m][c], v.u0[m][c], (-dtdx * du0 - dtdy * du1), c0, c1);
+    }
+  }
+  if (cj) {
+    const double du = d4<ODR>(v.ez, c, sy);
+    v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+  }
+  if (ci) {
+    const double du = d4<ODR>(v.ez, c, 1);
+    v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+  }
+}
+
+__global__ void k_dbound(View v, const DCtl *dc, int nc)
+{
+  QAS_DSUB_GUARD();
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    int si, sj, sk;
+    double fac;
+    gather_src(v, 0, m, i, j, k, si, sj, sk, fac);
+    if (si != i || sj != j || sk != k) {
+      double *u = v.u[m];
+      u[c] = fac * u[cidx(g, si, sj, sk)];
+    }
+  }
+}
+
+// ut = u at the start of each dsptv call
+__global__ void k_dcopy(View v, const DCtl *dc, int nc)
+{
+  QAS_DSUB_GUARD();
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= v.g.nd) return;
+#pragma unroll
+  for (int m = 0; m < 8; m++) v.u0[m][c] = v.u[m][c];
+}
+
+}  // namespace qas

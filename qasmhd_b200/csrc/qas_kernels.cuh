@@ -1,0 +1,620 @@
+// qas_kernels.cuh -- kernels of one SSP-RK stage of the qasMHD step on sm_100a.
+//
+// Data layout in HBM (one pool per context): structure-of-arrays FP64, one
+// array per field in the reference's ghost-padded order ss = nx*(ny*k+j)+i,
+// so host<->device copies are single memcpys.  Per stage:
+//   k_prim      cell-centre B (with its ghost fill folded in as a gather) and
+//               primitives for every cell                     (mhd2d_solve.cpp:51-89)
+//   k_dv        shock detector dv with its ghost fill         (:105-125)  MLAU/LHLLD only
+//   k_lr        characteristic WCNS face states of each cell + CUCT induction states
+//   k_flux      Riemann flux per face, central/upwind split of the induction flux
+//   k_emf       corner EMFs with the CUCT weight computed in place
+//   k_update    SSP-RK combine of the cell-centred fields and the CT update of B
+//   k_bound     ghost fill of the state as a gather over precomputed per-axis maps
+#pragma once
+
+#include "qas_device.cuh"
+
+namespace qas {
+
+constexpr int GH = 4;  // ghost cells per side
+
+struct Geo {
+  int dim, nx, ny, nz;
+  long long nd;
+  long long s[3];  // strides of x, y, z
+  int n[3];        // extents incl. ghosts
+};
+
+// Device control block of the exec_ loop (dt, tim, n kept on the device).
+struct Ctl {
+  double dt;
+  double tim;
+  double tmax;
+  double dtd[3];                 // dt/dx, dt/dy, dt/dz of the current step
+  unsigned long long vmax_bits;  // setdt reduction (positive doubles order like their bits)
+  int n, nmax, done, first;
+  int err;                       // latched device error bits
+  int pad;
+};
+
+// Ghost-fill maps: for group G (0 state, 1 cell-centre B, 2 dv), field m, axis a and
+// index i along that axis: the source index and factor after all fill passes of that
+// axis (built on the host by replaying the reference's passes symbolically).
+struct Maps {
+  const int *src;
+  const double *fac;
+  int nmax;
+};
+
+struct View {
+  Geo g;
+  int rmn, odr, rk, ctw;
+  double gam;
+  double dx, dy, dz;
+  double *u[8];    // state ro,mx,my,mz,bx,by,bz,en
+  double *u0[8];   // state at the start of the step (ut)
+  double *vx, *vy, *vz, *pr, *cx, *cy, *cz;
+  double *dv[3];
+  double *vl[7], *vr[7];  // face states of each cell along the current axis
+  double *ql[2], *qr[2];  // induction-flux states
+  double *f[3][8];        // face fluxes per direction
+  double *fc[3][2];       // central parts of the induction fluxes per direction
+  double *ex, *ey, *ez;
+  Ctl *ctl;
+  Maps maps;
+};
+
+__device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
+{
+  return (long long)g.nx * ((long long)g.ny * k + j) + i;
+}
+
+__device__ __forceinline__ int map_src(const Maps &m, int G, int f, int a, int i)
+{
+  return m.src[((G * 8 + f) * 3 + a) * m.nmax + i];
+}
+__device__ __forceinline__ double map_fac(const Maps &m, int G, int f, int a, int i)
+{
+  return m.fac[((G * 8 + f) * 3 + a) * m.nmax + i];
+}
+
+// source cell and factor of (i,j,k) for group G / field f
+__device__ __forceinline__ void gather_src(const View &v, int G, int f, int i, int j, int k, int &si, int &sj, int &sk,
+                                           double &fac)
+{
+  si = map_src(v.maps, G, f, 0, i);
+  fac = map_fac(v.maps, G, f, 0, i);
+  sj = j;
+  sk = k;
+  if (v.g.dim >= 2) {
+    sj = map_src(v.maps, G, f, 1, j);
+    fac = fac * map_fac(v.maps, G, f, 1, j);
+  }
+  if (v.g.dim >= 3) {
+    sk = map_src(v.maps, G, f, 2, k);
+    fac = fac * map_fac(v.maps, G, f, 2, k);
+  }
+}
+
+#define QAS_CELL_INDEX()                                   \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;     \
+  const int j = blockIdx.y;                                \
+  const int k = blockIdx.z;                                \
+  if (i >= v.g.nx) return;
+
+// ---------------------------------------------------------------------------
+// primitives + cell-centre B (prmtv, bcell/bb2cc + bound(cx,cy,cz))
+// ---------------------------------------------------------------------------
+template <int ODR>
+__global__ void k_prim(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+  double cx, cy, cz;
+  if (g.dim == 1) {
+    cx = v.u[4][c];
+    cy = v.u[5][c];
+    cz = v.u[6][c];
+  } else {
+    int si, sj, sk;
+    double fac;
+    gather_src(v, 1, 0, i, j, k, si, sj, sk, fac);
+    long long s = cidx(g, si, sj, sk);
+    const double *bx = v.u[4];
+    cx = fac * fcen<ODR>(bx[s - 1], bx[s], bx[s + 1], bx[s + 2]);
+    gather_src(v, 1, 1, i, j, k, si, sj, sk, fac);
+    s = cidx(g, si, sj, sk);
+    const double *by = v.u[5];
+    const long long sy = g.s[1];
+    cy = fac * fcen<ODR>(by[s - sy], by[s], by[s + sy], by[s + 2 * sy]);
+    if (g.dim == 3) {
+      gather_src(v, 1, 2, i, j, k, si, sj, sk, fac);
+      s = cidx(g, si, sj, sk);
+      const double *bz = v.u[6];
+      const long long sz = g.s[2];
+      cz = fac * fcen<ODR>(bz[s - sz], bz[s], bz[s + sz], bz[s + 2 * sz]);
+    } else {
+      cz = v.u[6][c];
+    }
+  }
+  const double ro = v.u[0][c];
+  const double iro = 1.0 / ro;
+  const double vx = v.u[1][c] * iro;
+  const double vy = v.u[2][c] * iro;
+  const double vz = v.u[3][c] * iro;
+  const double v2 = vx * vx + vy * vy + vz * vz;
+  const double b2 = cx * cx + cy * cy + cz * cz;
+  const double pr = (v.gam - 1) * (v.u[7][c] - 0.5 * (ro * v2 + b2));
+  v.vx[c] = vx;
+  v.vy[c] = vy;
+  v.vz[c] = vz;
+  v.pr[c] = pr;
+  v.cx[c] = cx;
+  v.cy[c] = cy;
+  v.cz[c] = cz;
+  // latch a device error for a broken interior state (results are not altered)
+  bool interior = i >= GH && i < g.nx - GH && (g.dim < 2 || (j >= GH && j < g.ny - GH)) &&
+                  (g.dim < 3 || (k >= GH && k < g.nz - GH));
+  if (interior && !(ro > 0.0 && pr > 0.0 && isfinite(vx) && isfinite(vy) && isfinite(vz))) atomicOr(&v.ctl->err, 1);
+}
+
+// ---------------------------------------------------------------------------
+// shock detector dv (mhd2d_solve.cpp:105-125, mhd3d_solve.cpp:138-164)
+// ---------------------------------------------------------------------------
+__global__ void k_dv(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+  const double *vel[3] = {v.vx, v.vy, v.vz};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (a >= g.dim) break;
+    int si, sj, sk;
+    double fac;
+    gather_src(v, 2, a, i, j, k, si, sj, sk, fac);
+    const long long s = cidx(g, si, sj, sk);
+    const long long st = g.s[a];
+    const double *p = vel[a];
+    const double raw = qmin((p[s + st] - p[s]), (p[s] - p[s - st]));
+    v.dv[a][c] = fac * raw;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face states of each cell along axis A (mhd_lrstate + mhd_lr_fb)
+// ---------------------------------------------------------------------------
+template <int ODR, int A>
+__global__ void __launch_bounds__(128) k_lr(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const int pos = A == 0 ? i : (A == 1 ? j : k);
+  const int n = g.n[A];
+  if (pos < 2 || pos >= n - 2) return;
+  const long long c = cidx(g, i, j, k);
+  const long long s = g.s[A];
+  constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+  const double *vn = A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
+  const double *vb = B == 0 ? v.vx : (B == 1 ? v.vy : v.vz);
+  const double *vc = C == 0 ? v.vx : (C == 1 ? v.vy : v.vz);
+  const double *cn = A == 0 ? v.cx : (A == 1 ? v.cy : v.cz);
+  const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
+  const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
+  const double *bnf = v.u[4 + A];
+  double q[7][5];
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    const long long p = c + (m - 2) * s;
+    q[0][m] = v.u[0][p];
+    q[1][m] = vn[p];
+    q[2][m] = vb[p];
+    q[3][m] = vc[p];
+    q[4][m] = cb[p];
+    q[5][m] = ccp[p];
+    q[6][m] = v.pr[p];
+  }
+  double vl[7], vr[7];
+  face_states<ODR>(q, cn[c], v.gam, vl, vr);
+#pragma unroll
+  for (int m = 0; m < 7; m++) {
+    v.vl[m][c] = vl[m];
+    v.vr[m][c] = vr[m];
+  }
+  if (g.dim >= 2) {
+    const double bfl = bnf[c + s], bfr = bnf[c];
+    // transverse component t0 = B axis (used in 3D; in 2D along x), t1 = C axis (3D; 2D along y)
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      if (g.dim == 2 && ((A == 0 && t == 1) || (A == 1 && t == 0))) continue;
+      const double *vt = t == 0 ? vb : vc;
+      const double *bt = t == 0 ? cb : ccp;
+      double prod[5], vts[5];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        const long long p = c + (m - 2) * s;
+        prod[m] = bt[p] * vn[p];
+        vts[m] = vt[p];
+      }
+      double fl0, fr0, fl1, fr1;
+      lin_lr<ODR>(prod, fl0, fr0);
+      lin_lr<ODR>(vts, fl1, fr1);
+      v.ql[t][c] = fl0 - bfl * fl1;
+      v.qr[t][c] = fr0 - bfr * fr1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann flux per face along axis A (mhd2d_solve.cpp:172-199 and 3D analogues)
+// ---------------------------------------------------------------------------
+template <int RMN, int A>
+__global__ void __launch_bounds__(128) k_flux(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const int pos = A == 0 ? i : (A == 1 ? j : k);
+  const int n = g.n[A];
+  if (pos < 3 || pos >= n - 2) return;
+  const long long f = cidx(g, i, j, k);
+  const long long s = g.s[A];
+  constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+  double L[7], R[7], F[7];
+#pragma unroll
+  for (int m = 0; m < 7; m++) {
+    L[m] = v.vl[m][f - s];
+    R[m] = v.vr[m][f];
+  }
+  const double bnf = v.u[4 + A][f];
+  const double bn = 0.5 * (bnf + bnf);
+  double dv0 = 0.0, dv1 = 0.0;
+  if (RMN >= 2) {
+    const double *vn = A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
+    dv0 = vn[f] - vn[f - s];
+    if (g.dim == 2) {
+      const double *dt = v.dv[A == 0 ? 1 : 0];
+      dv1 = qmin(dt[f - s], dt[f]);
+    } else if (g.dim == 3) {
+      const double *d1 = v.dv[B], *d2 = v.dv[C];
+      dv1 = qmin(qmin(d1[f - s], d1[f]), qmin(d2[f - s], d2[f]));
+    }
+  }
+  riemann<RMN>(L, R, bn, v.gam, dv0, dv1, F);
+  v.f[A][0][f] = F[0];
+  v.f[A][1 + A][f] = F[1];
+  v.f[A][1 + B][f] = F[2];
+  v.f[A][1 + C][f] = F[3];
+  double fbt = F[4], fbu = F[5];
+  if (g.dim >= 2) {
+    if (g.dim == 3 || A == 0) {
+      const double fc0 = 0.5 * (v.ql[0][f - s] + v.qr[0][f]);
+      v.fc[A][0][f] = fc0;
+      fbt -= fc0;
+    }
+    if (g.dim == 3 || A == 1) {
+      const double fc1 = 0.5 * (v.ql[1][f - s] + v.qr[1][f]);
+      v.fc[A][1][f] = fc1;
+      fbu -= fc1;
+    }
+  }
+  v.f[A][4 + B][f] = fbt;
+  v.f[A][4 + C][f] = fbu;
+  v.f[A][7][f] = F[6];
+}
+
+// ---------------------------------------------------------------------------
+// corner EMFs (mhd2d_solve.cpp:201-232, :308-339; mhd3d_solve.cpp:259-328,
+// :423-492, :587-656) with the CUCT weight (mhd_func.c:56-76) computed here.
+// ---------------------------------------------------------------------------
+template <int ODR>
+__device__ __forceinline__ double emf_term(const double *up, const double *cen, long long c, long long s, double sgn,
+                                           double wgt)
+{
+  double a[5], b[5];
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    a[m] = up[c + (m - 3) * s];
+    b[m] = up[c + (m - 2) * s];
+  }
+  const double l0 = lin_left<ODR>(a), r0 = lin_right<ODR>(b);
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    a[m] = cen[c + (m - 3) * s];
+    b[m] = cen[c + (m - 2) * s];
+  }
+  const double l1 = lin_left<ODR>(a), r1 = lin_right<ODR>(b);
+  return sgn * ((l0 + r0) + wgt * (l1 + r1));
+}
+
+__device__ __forceinline__ double cuct_at(const View &v, const double *va, const double *vb, const double *ba,
+                                          const double *bb, long long c, long long oa, long long ob)
+{
+  if (!v.ctw) return 0.5;
+  const double *ro = v.u[0];
+  return cuct_weight(ro[c - oa - ob], ro[c - ob], ro[c - oa], ro[c], va[c - oa - ob], va[c - ob], va[c - oa], va[c],
+                     vb[c - oa - ob], vb[c - ob], vb[c - oa], vb[c], ba[c - ob], ba[c], bb[c - oa], bb[c]);
+}
+
+template <int ODR>
+__global__ void k_emf(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+  const long long sx = 1, sy = g.s[1], sz = g.s[2];
+  const bool ii = i >= 3 && i < g.nx - 2, jj = j >= 3 && j < g.ny - 2;
+  if (g.dim == 2) {
+    if (ii && jj) {
+      const double ct = cuct_at(v, v.vx, v.vy, v.u[4], v.u[5], c, sx, sy);
+      double ez = 0.0;
+      ez += emf_term<ODR>(v.f[0][5], v.fc[0][0], c, sy, -0.5, (1.0 - ct));
+      ez += emf_term<ODR>(v.f[1][4], v.fc[1][1], c, sx, +0.5, ct);
+      v.ez[c] = ez;
+    }
+    return;
+  }
+  const bool kk = k >= 3 && k < g.nz - 2;
+  if (ii && jj) {
+    const double ct0 = cuct_at(v, v.vx, v.vy, v.u[4], v.u[5], c, sx, sy);
+    double ez = 0.0;
+    ez += emf_term<ODR>(v.f[0][5], v.fc[0][0], c, sy, -0.5, (1.0 - ct0));
+    ez += emf_term<ODR>(v.f[1][4], v.fc[1][1], c, sx, +0.5, ct0);
+    v.ez[c] = ez;
+  }
+  if (ii && kk) {
+    const double ct2 = cuct_at(v, v.vz, v.vx, v.u[6], v.u[4], c, sz, sx);
+    double ey = 0.0;
+    ey += emf_term<ODR>(v.f[0][6], v.fc[0][1], c, sz, +0.5, ct2);
+    ey += emf_term<ODR>(v.f[2][4], v.fc[2][0], c, sx, -0.5, (1.0 - ct2));
+    v.ey[c] = ey;
+  }
+  if (jj && kk) {
+    const double ct1 = cuct_at(v, v.vy, v.vz, v.u[5], v.u[6], c, sy, sz);
+    double ex = 0.0;
+    ex += emf_term<ODR>(v.f[1][6], v.fc[1][0], c, sz, -0.5, (1.0 - ct1));
+    ex += emf_term<ODR>(v.f[2][5], v.fc[2][1], c, sy, +0.5, ct1);
+    v.ex[c] = ex;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SSP-RK combine + CT update (mhd_updt1d/2d/3d, mhd_updt2d_ctb/3d_ctb:
+// common/mhd_func.c:207-325)
+// ---------------------------------------------------------------------------
+template <int ODR>
+__device__ __forceinline__ double d4(const double *p, long long c, long long s)
+{
+  return dfc<ODR>(p[c - s], p[c], p[c + s], p[c + 2 * s]);
+}
+
+template <int ODR>
+__global__ void k_update(View v, double c0, double c1)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
+  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
+  if (i > g.nx - GH) return;
+  const long long c = cidx(g, i, j, k);
+  const double dtdx = v.ctl->dtd[0], dtdy = v.ctl->dtd[1], dtdz = v.ctl->dtd[2];
+  const bool ci = i < g.nx - GH;
+  const bool cj = g.dim < 2 || j < g.ny - GH;
+  const bool ck = g.dim < 3 || k < g.nz - GH;
+  const long long sy = g.s[1], sz = g.s[2];
+  if (ci && cj && ck) {
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (m == 4) continue;
+      if (g.dim >= 2 && m == 5) continue;
+      if (g.dim >= 3 && m == 6) continue;
+      double du;
+      const double du0 = d4<ODR>(v.f[0][m], c, 1);
+      if (g.dim == 1) {
+        du = -dtdx * du0;
+      } else {
+        const double du1 = d4<ODR>(v.f[1][m], c, sy);
+        if (g.dim == 2) {
+          du = (-dtdx * du0 - dtdy * du1);
+        } else {
+          const double du2 = d4<ODR>(v.f[2][m], c, sz);
+          du = (-dtdx * du0 - dtdy * du1 - dtdz * du2);
+        }
+      }
+      v.u[m][c] = rk_combine(v.u[m][c], v.u0[m][c], du, c0, c1);
+    }
+  }
+  if (g.dim == 2) {
+    if (cj) {  // bx on i in [GH, nx-GH]
+      const double du = d4<ODR>(v.ez, c, sy);
+      v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+    }
+    if (ci && j <= g.ny - GH) {  // by on j in [GH, ny-GH]
+      const double du = d4<ODR>(v.ez, c, 1);
+      v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+    }
+  } else if (g.dim == 3) {
+    if (ck && cj) {
+      const double du0 = +d4<ODR>(v.ez, c, sy);
+      const double du1 = -d4<ODR>(v.ey, c, sz);
+      v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
+    }
+    if (ck && ci) {
+      const double du0 = +d4<ODR>(v.ex, c, sz);
+      const double du1 = -d4<ODR>(v.ez, c, 1);
+      v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
+    }
+    if (cj && ci) {
+      const double du0 = +d4<ODR>(v.ey, c, 1);
+      const double du1 = -d4<ODR>(v.ex, c, sy);
+      v.u[6][c] = rk_combine(v.u[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ghost fill of the state (bound())
+// ---------------------------------------------------------------------------
+__global__ void k_bound(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    int si, sj, sk;
+    double fac;
+    gather_src(v, 0, m, i, j, k, si, sj, sk, fac);
+    if (si != i || sj != j || sk != k) {
+      double *u = v.u[m];
+      u[c] = fac * u[cidx(g, si, sj, sk)];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// exec_ loop control and setdt
+// ---------------------------------------------------------------------------
+// begin of a loop iteration: the while() test of exec_, tim += dt, dt/dx
+__global__ void k_begin_step(View v, int check_tim)
+{
+  Ctl *c = v.ctl;
+  if (c->done) return;
+  const bool go = check_tim ? (c->n < c->nmax && c->tim < c->tmax) : (c->n < c->nmax);
+  if (!go) {
+    c->done = 1;
+    return;
+  }
+  c->n += 1;
+  c->tim += c->dt;
+  c->dtd[0] = c->dt / v.dx;
+  c->dtd[1] = v.g.dim >= 2 ? c->dt / v.dy : 0.0;
+  c->dtd[2] = v.g.dim >= 3 ? c->dt / v.dz : 0.0;
+}
+
+// dt/dx etc. for a host-supplied dt (qas_step)
+__global__ void k_set_dt(View v, double dt)
+{
+  Ctl *c = v.ctl;
+  c->dt = dt;
+  c->dtd[0] = dt / v.dx;
+  c->dtd[1] = v.g.dim >= 2 ? dt / v.dy : 0.0;
+  c->dtd[2] = v.g.dim >= 3 ? dt / v.dz : 0.0;
+}
+
+__global__ void k_vmax_reset(View v)
+{
+  if (v.ctl->done) return;
+  v.ctl->vmax_bits = (unsigned long long)__double_as_longlong(1.0);
+}
+
+// max over the interior of |v| + c_f with B from the 2nd-order face average
+// (mhd2d_class.cpp:17-26); NaN never wins, as with `if (vtmp > vmax)`.
+__global__ void k_vmax(View v)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
+  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
+  double best = 1.0;
+  if (i < g.nx - GH) {
+    const long long c = cidx(g, i, j, k);
+    double cx, cy, cz;
+    if (g.dim == 1) {
+      cx = v.u[4][c];
+      cy = v.u[5][c];
+      cz = v.u[6][c];
+    } else {
+      cx = 0.5 * (v.u[4][c] + v.u[4][c + 1]);
+      cy = 0.5 * (v.u[5][c] + v.u[5][c + g.s[1]]);
+      cz = g.dim == 3 ? 0.5 * (v.u[6][c] + v.u[6][c + g.s[2]]) : v.u[6][c];
+    }
+    const double ro = v.u[0][c];
+    const double iro = 1.0 / ro;
+    const double vx = v.u[1][c] * iro, vy = v.u[2][c] * iro, vz = v.u[3][c] * iro;
+    const double v2 = vx * vx + vy * vy + vz * vz;
+    const double b2 = cx * cx + cy * cy + cz * cz;
+    const double pr = (v.gam - 1) * (v.u[7][c] - 0.5 * (ro * v2 + b2));
+    const double vf = sqrt((v.gam * pr + (cx * cx + cy * cy + cz * cz)) / ro);
+    double vt;
+    if (g.dim == 1)
+      vt = fabs(vx) + vf;
+    else if (g.dim == 2)
+      vt = sqrt(vx * vx + vy * vy) + vf;
+    else
+      vt = sqrt(vx * vx + vy * vy + vz * vz) + vf;
+    if (vt > best) best = vt;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, best, o);
+    best = (other > best) ? other : best;
+  }
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = best;
+  __syncthreads();
+  if (wid == 0) {
+    best = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 1.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, best, o);
+      best = (other > best) ? other : best;
+    }
+    if (lane == 0) atomicMax(&v.ctl->vmax_bits, (unsigned long long)__double_as_longlong(best));
+  }
+}
+
+// dt = cfl*dr/vmax; on the first call also exec_'s nmax (mhd2d_class.cpp:27-32,
+// mhd1d_class.cpp:146-151)
+__global__ void k_setdt(View v, double cfl, double dr, int rule, double dtrec, int nout)
+{
+  Ctl *c = v.ctl;
+  if (c->done) return;
+  const double vmax = __longlong_as_double((long long)c->vmax_bits);
+  c->dt = cfl * dr / vmax;
+  if (c->first) {
+    if (rule == 2) {
+      const int nrec = (int)(dtrec / c->dt + 0.5);
+      c->nmax = nrec * nout;
+    } else if (rule == 1) {
+      c->nmax = (int)(c->tmax / c->dt + 0.5);
+    }
+    c->first = 0;
+  }
+}
+
+// |div B| with df1[ODR-1] over the interior; max by bit pattern of non-negative doubles
+template <int ODR>
+__global__ void k_divb(View v, unsigned long long *out)
+{
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
+  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
+  double d = 0.0;
+  if (i < g.nx - GH && g.dim >= 2) {
+    const long long c = cidx(g, i, j, k);
+    double s = d4<ODR>(v.u[4], c, 1) / v.dx + d4<ODR>(v.u[5], c, g.s[1]) / v.dy;
+    if (g.dim == 3) s += d4<ODR>(v.u[6], c, g.s[2]) / v.dz;
+    d = fabs(s);
+    if (!(d == d)) d = __longlong_as_double(0x7ff0000000000000LL);  // NaN reports as +inf
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, d, o);
+    d = (other > d) ? other : d;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(d));
+}
+
+}  // namespace qas

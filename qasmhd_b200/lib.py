@@ -1,0 +1,274 @@
+"""ctypes binding of libqas.so (include/qas.h).
+
+The shared library is built in-tree (``qasmhd_b200/libqas.so``) by
+:func:`qasmhd_b200.build.build_library`.  Loading fails loudly when it is
+missing: there is no CPU fallback for the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqas.so")
+
+# qas_status values
+QAS_OK = 0
+QAS_ERR_INVALID = 1
+QAS_ERR_CUDA = 2
+QAS_ERR_NOMEM = 3
+QAS_ERR_NONFINITE = 4
+QAS_ERR_TIMEOUT = 5
+QAS_ERR_UNSUPPORTED = 6
+QAS_ERR_NO_DEVICE = 7
+
+# every exported entry point of include/qas.h (checked by the CPU tests)
+EXPORTS = (
+    "qas_status_str", "qas_abi_version", "qas_last_cuda_error", "qas_create", "qas_destroy",
+    "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
+    "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
+    "qas_run", "qas_run_reset", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
+    "qas_kernel_launches", "qas_bc_map",
+)
+
+
+class QasError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        self.status = status
+        msg = f"{what}: qas status {status}"
+        if _lib is not None:
+            msg += f" ({_lib.qas_status_str(status).decode()})"
+        if detail:
+            msg += f" [{detail}]"
+        super().__init__(msg)
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("nxm", ctypes.c_int), ("nym", ctypes.c_int), ("nzm", ctypes.c_int),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+                ("gam", ctypes.c_double)]
+
+
+class Scheme(ctypes.Structure):
+    _fields_ = [("rmn", ctypes.c_int), ("odr", ctypes.c_int), ("rk", ctypes.c_int), ("ctw", ctypes.c_int)]
+
+
+class BC(ctypes.Structure):
+    _fields_ = [("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8)]
+
+
+class RunOpts(ctypes.Structure):
+    _fields_ = [("max_steps", ctypes.c_int), ("flg", ctypes.c_int), ("stop_rule", ctypes.c_int),
+                ("cfl", ctypes.c_double), ("dtrec", ctypes.c_double), ("nout", ctypes.c_int),
+                ("use_graph", ctypes.c_int), ("nu0", ctypes.c_double), ("eta0", ctypes.c_double)]
+
+
+class RunInfo(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int), ("n", ctypes.c_int), ("nmax", ctypes.c_int),
+                ("tim", ctypes.c_double), ("dt", ctypes.c_double)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libqas.so (once) and declare the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m qasmhd_b200.build` "
+                                "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    st = ctypes.c_int
+    lib.qas_status_str.argtypes = [st]
+    lib.qas_status_str.restype = ctypes.c_char_p
+    lib.qas_abi_version.restype = ctypes.c_int
+    lib.qas_last_cuda_error.restype = ctypes.c_char_p
+    lib.qas_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Grid), ctypes.POINTER(Scheme),
+                               ctypes.POINTER(BC), ctypes.c_int]
+    lib.qas_destroy.argtypes = [vp]
+    lib.qas_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.qas_upload.argtypes = [vp, ctypes.POINTER(dp)]
+    lib.qas_download.argtypes = [vp, ctypes.POINTER(dp)]
+    lib.qas_upload_block.argtypes = [vp, dp]
+    lib.qas_download_block.argtypes = [vp, dp]
+    lib.qas_device_state.argtypes = [vp, ctypes.POINTER(dp)]
+    lib.qas_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.qas_bound.argtypes = [vp]
+    lib.qas_step.argtypes = [vp, ctypes.c_double]
+    lib.qas_cfl_vmax.argtypes = [vp, dp]
+    lib.qas_cfl_dt.argtypes = [vp, ctypes.c_double, dp]
+    lib.qas_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
+    lib.qas_run_reset.argtypes = [vp]
+    lib.qas_dissipate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.qas_dsptv.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.qas_max_divb.argtypes = [vp, dp]
+    lib.qas_sync.argtypes = [vp]
+    lib.qas_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
+    for name in EXPORTS:
+        if name not in ("qas_status_str", "qas_abi_version", "qas_last_cuda_error"):
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _check(status: int, what: str) -> None:
+    if status != QAS_OK:
+        detail = ""
+        if status in (QAS_ERR_CUDA, QAS_ERR_NOMEM) and _lib is not None:
+            detail = _lib.qas_last_cuda_error().decode()
+        raise QasError(status, what, detail)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Context:
+    """One device simulation: a qas_ctx handle with numpy-friendly calls."""
+
+    def __init__(self, dim: int, nxm: int, nym: int, nzm: int, dx: float, dy: float, dz: float, gam: float,
+                 rmn: int, odr: int, rk: int, ctw: int, dnx: Sequence[int], dny: Sequence[int],
+                 dnz: Sequence[int], device: int = -1):
+        self.lib = load()
+        g = Grid(dim, nxm, nym if dim >= 2 else 1, nzm if dim >= 3 else 1, dx, dy if dim >= 2 else 0.0,
+                 dz if dim >= 3 else 0.0, gam)
+        s = Scheme(rmn, odr, rk, ctw)
+        b = BC()
+        for m in range(8):
+            b.dnx[m], b.dny[m], b.dnz[m] = int(dnx[m]), int(dny[m]), int(dnz[m])
+        h = ctypes.c_void_p()
+        _check(self.lib.qas_create(ctypes.byref(h), ctypes.byref(g), ctypes.byref(s), ctypes.byref(b), device),
+               "qas_create")
+        self.h = h
+        nd = ctypes.c_longlong()
+        _check(self.lib.qas_cells(self.h, ctypes.byref(nd)), "qas_cells")
+        self.nd = int(nd.value)
+        self.dim = dim
+
+    @classmethod
+    def from_problem(cls, prob, device: int = -1) -> "Context":
+        return cls(prob.dim, prob.nxm, prob.nym, prob.nzm, prob.dx, prob.dy if prob.dim >= 2 else 0.0,
+                   prob.dz if prob.dim >= 3 else 0.0, prob.gam, prob.rmn, prob.odr, prob.rk, prob.ctw,
+                   prob.dnx, prob.dny, prob.dnz, device)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.qas_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # state transfer -------------------------------------------------------
+    def upload(self, state: np.ndarray) -> None:
+        st = np.ascontiguousarray(state, dtype=np.float64).reshape(8, -1)
+        assert st.shape[1] == self.nd, (st.shape, self.nd)
+        _check(self.lib.qas_upload_block(self.h, _dptr(st)), "qas_upload_block")
+
+    def download(self, shape=None) -> np.ndarray:
+        out = np.empty((8, self.nd), dtype=np.float64)
+        _check(self.lib.qas_download_block(self.h, _dptr(out)), "qas_download_block")
+        return out if shape is None else out.reshape(shape)
+
+    def download_into(self, out: np.ndarray) -> None:
+        """Download into a caller-owned C-contiguous float64 buffer of 8*nd values (e.g. pinned)."""
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == 8 * self.nd
+        _check(self.lib.qas_download_block(self.h, _dptr(out)), "qas_download_block")
+
+    def upload_fields(self, fields: Sequence[np.ndarray]) -> None:
+        """Upload 8 separate host arrays (the reference's val[8] pointers)."""
+        arrs = [np.ascontiguousarray(f, dtype=np.float64).reshape(-1) for f in fields]
+        ptrs = (ctypes.POINTER(ctypes.c_double) * 8)(*[_dptr(a) for a in arrs])
+        _check(self.lib.qas_upload(self.h, ptrs), "qas_upload")
+
+    def download_fields(self, fields: Sequence[np.ndarray]) -> None:
+        for f in fields:
+            assert f.flags["C_CONTIGUOUS"] and f.dtype == np.float64 and f.size == self.nd
+        ptrs = (ctypes.POINTER(ctypes.c_double) * 8)(*[_dptr(f) for f in fields])
+        _check(self.lib.qas_download(self.h, ptrs), "qas_download")
+
+    # stepping --------------------------------------------------------------
+    def bound(self) -> None:
+        _check(self.lib.qas_bound(self.h), "qas_bound")
+
+    def step(self, dt: float) -> None:
+        _check(self.lib.qas_step(self.h, float(dt)), "qas_step")
+
+    def cfl_vmax(self) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.qas_cfl_vmax(self.h, ctypes.byref(v)), "qas_cfl_vmax")
+        return v.value
+
+    def cfl_dt(self, cfl: float) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.qas_cfl_dt(self.h, float(cfl), ctypes.byref(v)), "qas_cfl_dt")
+        return v.value
+
+    def run(self, max_steps: int = 0, flg: int = 1, stop_rule: int = 0, cfl: float = 0.4, dtrec: float = 1.0,
+            nout: int = 1, use_graph: bool = True, nu0: float = 0.0, eta0: float = 0.0) -> RunInfo:
+        o = RunOpts(int(max_steps), int(flg), int(stop_rule), float(cfl), float(dtrec), int(nout),
+                    1 if use_graph else 0, float(nu0), float(eta0))
+        info = RunInfo()
+        _check(self.lib.qas_run(self.h, ctypes.byref(o), ctypes.byref(info)), "qas_run")
+        return info
+
+    def run_reset(self) -> None:
+        _check(self.lib.qas_run_reset(self.h), "qas_run_reset")
+
+    def dissipate(self, dt: float, nu0: float, eta0: float) -> None:
+        _check(self.lib.qas_dissipate(self.h, float(dt), float(nu0), float(eta0)), "qas_dissipate")
+
+    def dsptv(self, dt: float, nu0: float, eta0: float) -> None:
+        _check(self.lib.qas_dsptv(self.h, float(dt), float(nu0), float(eta0)), "qas_dsptv")
+
+    def max_divb(self) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.qas_max_divb(self.h, ctypes.byref(v)), "qas_max_divb")
+        return v.value
+
+    def sync(self) -> None:
+        _check(self.lib.qas_sync(self.h), "qas_sync")
+
+    def kernel_launches(self) -> int:
+        v = ctypes.c_longlong()
+        _check(self.lib.qas_kernel_launches(self.h, ctypes.byref(v)), "qas_kernel_launches")
+        return int(v.value)
+
+    def stream(self) -> int:
+        v = ctypes.c_void_p()
+        _check(self.lib.qas_stream(self.h, ctypes.byref(v)), "qas_stream")
+        return int(v.value or 0)
+
+
+def bc_map(prob, group: int, field: int, axis: int):
+    """Host-only: the (source, factor) ghost-fill map of one group/field/axis (qas_bc_map)."""
+    lib = load()
+    g = Grid(prob.dim, prob.nxm, prob.nym if prob.dim >= 2 else 1, prob.nzm if prob.dim >= 3 else 1,
+             prob.dx, prob.dy if prob.dim >= 2 else 0.0, prob.dz if prob.dim >= 3 else 0.0, prob.gam)
+    b = BC()
+    for m in range(8):
+        b.dnx[m], b.dny[m], b.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+    n = (prob.nx, prob.ny, prob.nz)[axis]
+    src = np.zeros(n, dtype=np.int32)
+    fac = np.zeros(n, dtype=np.float64)
+    _check(lib.qas_bc_map(ctypes.byref(g), ctypes.byref(b), group, field, axis,
+                          src.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(fac), n), "qas_bc_map")
+    return src, fac

@@ -289,8 +289,6 @@ def smooth_wave(dim: int, n: int, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3
     by = 0.4 + amp * wave(5)
     bz = -0.3 + amp * wave(6)
     pr = 0.8 + amp * wave(7)
-    if dim < 3:
-        vz = vz * 1.0
     st = _pack(ro, vx, vy, vz, bx, by, bz, pr, bx, by, bz, p.gam)
     p.state = st
     return p

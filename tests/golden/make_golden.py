@@ -1,0 +1,133 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+The reference ships no golden vectors or known-answer tests, so every fixture
+here is produced by running the reference's own code, compiled from its
+sources by oracle/Makefile (oracle/_ref/ref1d, ref2d_ctw*, ref3d_ctw*,
+ref_kat).  Inputs are regenerated deterministically by qasmhd_b200.problems
+and numpy seeds; the fixtures store the outputs plus a SHA-256 of each input
+so a drift of the generators is caught.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import refcase as R  # noqa: E402
+from qasmhd_b200 import problems as P  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+# ---------------------------------------------------------------------------
+# point-function inputs (also used by the tests to rebuild the same inputs)
+# ---------------------------------------------------------------------------
+
+def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+
+    def states(m):
+        ro = rng.uniform(0.1, 2.0, m)
+        v = rng.normal(0.0, 1.0, (m, 3))
+        b = rng.normal(0.0, 1.0, (m, 2))
+        pr = rng.uniform(0.05, 2.0, m)
+        return np.column_stack([ro, v, b, pr])
+
+    if kind == "flux":
+        a = np.column_stack([states(n), states(n), rng.normal(0, 1, n), np.full(n, 5.0 / 3.0),
+                             rng.normal(0, 0.5, (n, 2))])
+        a[::9, 14] = 0.0          # Bn = 0
+        a[1::9, 7:14] = a[1::9, 0:7]  # identical left/right states
+        return a
+    if kind == "interp":
+        a = rng.normal(0, 1, (n, 5))
+        a[::7] = a[::7, :1]       # constant stencils
+        return a
+    if kind == "lrstate":
+        ro = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.1
+        rest = rng.normal(0, 1, (n, 25))
+        pr = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.05
+        a = np.concatenate([ro, rest, pr, rng.normal(0, 1, (n, 1)), np.full((n, 1), 5.0 / 3.0)], axis=1)
+        a[::7, 5:10] = 0.0        # exactly-zero normal velocity stencils
+        a[3::7, 25:30] = 0.0      # exactly-zero bu stencils
+        a[5::11, 5:10] *= 8.0     # supersonic centres (fast-mode eigenvectors)
+        return a
+    if kind == "cuct":
+        return np.concatenate([np.abs(rng.normal(1, 0.2, (n, 4))) + 0.1, rng.normal(0, 1, (n, 16))], axis=1)
+    raise ValueError(kind)
+
+
+KAT_FUNCS = {"flux": ([0, 1, 2, 3], 7), "interp": (list(range(10, 20)), 2), "lrstate": ([20, 21, 22, 23], 14),
+             "cuct": ([30], 1)}
+
+
+# ---------------------------------------------------------------------------
+# step cases: (name, builder, mode, nsteps)
+# ---------------------------------------------------------------------------
+
+def _kh2_eta():
+    p = P.kelvin_helmholtz(2, 16, mach=0.3, rmn=P.RMN_ROE)
+    p.eta0 = 1e-3
+    p.nu0 = 5e-4
+    return p
+
+
+def _wave_bc(dim, seed):
+    rng = np.random.default_rng(seed)
+
+    def flags():
+        f = [int(rng.choice([-2, -1, 1, 2])) for _ in range(8)]
+        f[0] = int(rng.choice([1, 2]))
+        f[7] = int(rng.choice([1, 2]))
+        return tuple(f)
+
+    dn = tuple(flags() if a < dim and rng.random() < 0.7 else (0,) * 8 for a in range(3))
+    return P.smooth_wave(dim, 12 if dim < 3 else 6, dn=dn, rmn=seed % 4)
+
+
+STEP_CASES = [
+    *[(f"bw1d_rmn{r}", (lambda r=r: P.brio_wu(64, rmn=r)), R.MODE_RUN, 5) for r in range(4)],
+    *[(f"bw1d_odr{o}", (lambda o=o: P.brio_wu(64, odr=o, rk=min(o, 3))), R.MODE_RUN, 5) for o in (1, 2, 3)],
+    ("bw1d_exec", lambda: P.brio_wu(64, tmax=0.02), R.MODE_EXEC, 0),
+    *[(f"ot2d_rmn{r}", (lambda r=r: P.orszag_tang(16, rmn=r)), R.MODE_RUN, 3) for r in range(4)],
+    ("ot2d_ctw0", lambda: P.orszag_tang(16, ctw=0), R.MODE_RUN, 3),
+    *[(f"ot2d_odr{o}", (lambda o=o: P.orszag_tang(16, odr=o, rk=min(o, 3))), R.MODE_RUN, 3) for o in (1, 2, 3)],
+    ("ot2d_exec", lambda: P.orszag_tang(16, tmax=0.05), R.MODE_EXEC, 0),
+    ("kh2d_mlau", lambda: P.kelvin_helmholtz(2, 16, mach=0.3, rmn=P.RMN_MLAU), R.MODE_RUN, 3),
+    ("kh2d_roe_eta", _kh2_eta, R.MODE_DRUN, 3),
+    *[(f"kh3d_rmn{r}", (lambda r=r: P.kelvin_helmholtz(3, 6, mach=0.3, rmn=r)), R.MODE_RUN, 2) for r in range(4)],
+    *[(f"wave{d}d_bc{s}", (lambda d=d, s=s: _wave_bc(d, s)), R.MODE_RUN, 2) for d in (1, 2, 3) for s in (1, 2)],
+]
+
+
+def main() -> None:
+    for name, (funcs, nout) in KAT_FUNCS.items():
+        inp = kat_inputs(name)
+        outs = {f"f{f}": R.run_kat(f, inp, nout) for f in funcs}
+        np.savez_compressed(os.path.join(OUT, f"kat_{name}.npz"), input_sha=sha(inp), **outs)
+        print("kat", name, inp.shape)
+    data = {}
+    for name, build, mode, nsteps in STEP_CASES:
+        p = build()
+        r = R.run_reference(p, mode, nsteps=nsteps, nthreads=4)
+        data[f"{name}__state"] = r["state"]
+        data[f"{name}__dts"] = r["dts"]
+        data[f"{name}__meta"] = np.array([r["steps"], r["tim"], r["dt"]])
+        data[f"{name}__insha"] = np.array(sha(p.state))
+        print("step", name, p.nd, r["steps"])
+    np.savez_compressed(os.path.join(OUT, "steps.npz"), **data)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,67 @@
+"""Pin the plain-C oracle (oracle/qas_oracle.c) to the reference.
+
+* against the committed golden fixtures, which were produced by the reference's
+  own code compiled from its sources (tests/golden/make_golden.py);
+* against the live reference binaries (oracle/_ref) when they are present.
+Everything is compared bit-for-bit (== semantics).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import refcase as R
+from qasmhd_b200 import problems as P
+from tests.cases import assert_bitwise
+from tests.golden import make_golden as G
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("kind", sorted(G.KAT_FUNCS))
+def test_kat_golden(restatement, kind):
+    funcs, nout = G.KAT_FUNCS[kind]
+    inp = G.kat_inputs(kind)
+    gold = np.load(os.path.join(GOLD, f"kat_{kind}.npz"))
+    assert str(gold["input_sha"]) == G.sha(inp), "golden inputs drifted"
+    for f in funcs:
+        assert_bitwise(restatement.kat(f, inp, nout), gold[f"f{f}"], f"kat {kind} f{f}")
+
+
+@pytest.mark.parametrize("case", G.STEP_CASES, ids=[c[0] for c in G.STEP_CASES])
+def test_steps_golden(restatement, golden_steps, case):
+    name, build, mode, nsteps = case
+    p = build()
+    assert str(golden_steps[f"{name}__insha"]) == G.sha(p.state), "golden input state drifted"
+    r = restatement.run(p, nsteps, mode=mode)
+    assert_bitwise(r["state"], golden_steps[f"{name}__state"], name)
+    assert_bitwise(r["dts"], golden_steps[f"{name}__dts"], name + " dts")
+    meta = golden_steps[f"{name}__meta"]
+    assert r["steps"] == int(meta[0])
+
+
+needs_ref = pytest.mark.skipif(not R.reference_available(2, 1), reason="reference oracle binaries not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(4))
+def test_live_reference_random(restatement, seed):
+    rng = np.random.default_rng(100 + seed)
+    dim = int(rng.integers(1, 4))
+    rmn = int(rng.integers(0, 4))
+    odr = int(rng.integers(1, 5))
+    ctw = int(rng.integers(0, 2))
+    n = {1: 40, 2: 14, 3: 6}[dim]
+    p = P.smooth_wave(dim, n, rmn=rmn, odr=odr, rk=int(rng.integers(1, 4)), ctw=ctw, seed=seed)
+    a = R.run_reference(p, R.MODE_RUN, nsteps=2, nthreads=2)
+    b = restatement.run(p, 2, mode=R.MODE_RUN)
+    assert_bitwise(b["state"], a["state"], f"dim{dim} rmn{rmn} odr{odr}")
+
+
+@needs_ref
+def test_live_reference_dissipative(restatement):
+    p = P.kelvin_helmholtz(2, 12, mach=0.2, rmn=P.RMN_HLLD)
+    p.nu0, p.eta0 = 1e-3, 2e-3
+    a = R.run_reference(p, R.MODE_DSTEP, dt=2e-3, nthreads=2)
+    b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
+    assert_bitwise(b["state"], a["state"], "dstep")

@@ -1,0 +1,177 @@
+"""Parity of the CUDA path (through the C-ABI) with the reference.
+
+Bit-exact (== semantics) comparisons:
+* every golden case (made by the reference's own code) on the same inputs;
+* the plain-C oracle at moderate sizes (2D 128^2, 3D 24^3) for every solver;
+* single ideal(dt) / dsptv(dt) calls and exec_ loop termination rules.
+At the benchmark sizes, size-independent properties: div B at round-off, mass
+conservation on periodic grids, determinism of repeated runs.
+"""
+import numpy as np
+import pytest
+
+from oracle import refcase as R
+from qasmhd_b200 import lib as L
+from qasmhd_b200 import problems as P
+from tests.cases import assert_bitwise, run_gpu
+from tests.golden import make_golden as G
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", G.STEP_CASES, ids=[c[0] for c in G.STEP_CASES])
+def test_golden_cases(golden_steps, case):
+    name, build, mode, nsteps = case
+    p = build()
+    r = run_gpu(p, mode, nsteps)
+    assert_bitwise(r["state"], golden_steps[f"{name}__state"], name)
+    assert r["steps"] == int(golden_steps[f"{name}__meta"][0])
+
+
+@pytest.mark.parametrize("rmn", range(4))
+@pytest.mark.parametrize("odr", [2, 4])
+def test_ot2d_vs_oracle(restatement, rmn, odr):
+    p = P.orszag_tang(96, rmn=rmn, odr=odr)
+    a = restatement.run(p, 6, mode=R.MODE_RUN)
+    b = run_gpu(p, R.MODE_RUN, 6)
+    assert_bitwise(b["state"], a["state"], f"ot rmn{rmn} odr{odr}")
+
+
+@pytest.mark.parametrize("rmn", range(4))
+def test_kh3d_vs_oracle(restatement, rmn):
+    p = P.kelvin_helmholtz(3, 20, mach=0.3, rmn=rmn, nym=16, nzm=12)
+    a = restatement.run(p, 3, mode=R.MODE_RUN)
+    b = run_gpu(p, R.MODE_RUN, 3)
+    assert_bitwise(b["state"], a["state"], f"kh3d rmn{rmn}")
+
+
+@pytest.mark.parametrize("ctw", [0, 1])
+@pytest.mark.parametrize("odr", [1, 3])
+def test_kh3d_ctw_odr(restatement, ctw, odr):
+    p = P.kelvin_helmholtz(3, 10, mach=0.5, rmn=P.RMN_MLAU, ctw=ctw, odr=odr, rk=2)
+    a = restatement.run(p, 2, mode=R.MODE_RUN)
+    b = run_gpu(p, R.MODE_RUN, 2)
+    assert_bitwise(b["state"], a["state"], f"kh3d ctw{ctw} odr{odr}")
+
+
+def test_single_ideal_step(restatement):
+    p = P.orszag_tang(40, rmn=P.RMN_LHLLD)
+    a = restatement.run(p, 1, mode=R.MODE_STEP, dt=0.01)
+    b = run_gpu(p, R.MODE_STEP, dt=0.01)
+    assert_bitwise(b["state"], a["state"], "step")
+
+
+def test_single_dsptv(restatement):
+    p = P.kelvin_helmholtz(2, 32, mach=0.2)
+    p.nu0, p.eta0 = 2e-3, 1e-3
+    a = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=3e-3)
+    b = run_gpu(p, R.MODE_DSTEP, dt=3e-3)
+    assert_bitwise(b["state"], a["state"], "dsptv")
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_graph_and_eager_agree(restatement, use_graph):
+    p = P.orszag_tang(48)
+    a = restatement.run(p, 7, mode=R.MODE_RUN)
+    b = run_gpu(p, R.MODE_RUN, 7, use_graph=use_graph)
+    assert_bitwise(b["state"], a["state"], f"graph={use_graph}")
+
+
+def test_exec_rule_2d(restatement):
+    p = P.orszag_tang(32, tmax=0.12)
+    a = restatement.run(p, 0, mode=R.MODE_EXEC)
+    b = run_gpu(p, R.MODE_EXEC)
+    assert b["steps"] == a["steps"]
+    assert b["tim"] == a["tim"]
+    assert_bitwise(b["state"], a["state"], "exec 2d")
+
+
+def test_exec_rule_1d(restatement):
+    p = P.brio_wu(128, tmax=0.03)
+    a = restatement.run(p, 0, mode=R.MODE_EXEC)
+    b = run_gpu(p, R.MODE_EXEC)
+    assert b["steps"] == a["steps"]
+    assert_bitwise(b["state"], a["state"], "exec 1d")
+
+
+def test_run_in_pieces_matches_one_call(restatement):
+    p = P.orszag_tang(32)
+    a = restatement.run(p, 9, mode=R.MODE_RUN)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        for k in (3, 1, 5):   # odd split exercises the graph parity handling
+            ctx.run(max_steps=k, flg=1, stop_rule=0, cfl=p.cfl)
+        out = ctx.download(p.state.shape)
+    assert_bitwise(out, a["state"], "pieces")
+
+
+def test_cfl_reduction_matches(restatement):
+    p = P.kelvin_helmholtz(3, 12, mach=0.4)
+    import ctypes
+    g = restatement.grid(p)
+    st = np.ascontiguousarray(p.state)
+    vm = restatement.lib.qo_cfl_dt(ctypes.byref(g), st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1.0)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(st)
+        assert ctx.cfl_vmax() == vm
+
+
+def test_invalid_bc_rejected_on_device():
+    p = P.smooth_wave(2, 8, dn=((3,) * 8, (0,) * 8, (0,) * 8))
+    with pytest.raises(L.QasError) as e:
+        L.Context.from_problem(p)
+    assert e.value.status == L.QAS_ERR_INVALID
+
+
+def test_nonfinite_state_is_reported():
+    p = P.orszag_tang(16)
+    st = p.state.copy()
+    st[0, 0, 10, 10] = -1.0   # negative density in the interior
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(st)
+        ctx.bound()
+        ctx.step(1e-3)
+        with pytest.raises(L.QasError) as e:
+            ctx.sync()
+        assert e.value.status == L.QAS_ERR_NONFINITE
+
+
+# ---------------------------------------------------------------------------
+# benchmark sizes: size-independent properties
+# ---------------------------------------------------------------------------
+
+def interior(p, a):
+    s = slice(4, -4)
+    if p.dim == 2:
+        return a[..., 0, s, s]
+    return a[..., s, s, s]
+
+
+def test_ot_1024_invariants():
+    p = P.orszag_tang(1024)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        d0 = ctx.max_divb()
+        m0 = interior(p, p.state)[0].sum()
+        info = ctx.run(max_steps=20, flg=1, stop_rule=0, cfl=p.cfl)
+        out = ctx.download(p.state.shape)
+        d1 = ctx.max_divb()
+    assert info.steps == 20
+    assert np.isfinite(out).all()
+    assert d0 < 1e-11 and d1 < 1e-11, (d0, d1)
+    m1 = interior(p, out)[0].sum()
+    assert abs(m1 - m0) / m0 < 1e-12
+
+
+def test_kh_256_determinism_and_divb():
+    p = P.kelvin_helmholtz(3, 256)
+    outs = []
+    for _ in range(2):
+        with L.Context.from_problem(p) as ctx:
+            ctx.upload(p.state)
+            ctx.run(max_steps=2, flg=1, stop_rule=0, cfl=p.cfl)
+            outs.append(ctx.download(p.state.shape))
+            d = ctx.max_divb()
+    assert np.isfinite(outs[0]).all()
+    assert_bitwise(outs[0], outs[1], "repeat")
+    assert d < 1e-10, d
