@@ -17,7 +17,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -33,8 +32,8 @@ ALG_BYTES_PER_CELL_UPDATE = 512  # 8 FP64 fields: stage 1 reads u^n, writes; sta
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "bw1d_1024"], default="ot2d_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -59,55 +58,55 @@ def make_problem(name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every few
+    milliseconds during the timed region (read-only queries)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.005):
         self.dev = device_index
-        self.rows = []
-        self.proc = None
+        self.period = period_s
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
         self.thread = None
+        self.ok = False
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
         except Exception:
-            self.proc = None
             return
 
-        def reader():
-            for line in self.proc.stdout:
-                self.rows.append([x.strip() for x in line.split(",")])
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, rs))
+                except Exception:
+                    pass
+                time.sleep(self.period)
 
-        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread = threading.Thread(target=loop, daemon=True)
         self.thread.start()
 
     def stop(self):
-        if self.proc is None:
+        if not self.ok:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        if self.thread:
-            self.thread.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            for k, nm in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        self._stop.set()
+        self.thread.join(timeout=2)
+        import pynvml
+        names = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted({nm for _, rs in self.samples for nm, bit in names.items() if rs & bit})
+        sm = [s for s, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sm)}
 
 
 def cpu_baseline(prob, steps=3, threads=None):

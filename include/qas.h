@@ -165,6 +165,25 @@ qas_status qas_sync(qas_ctx *ctx);
 qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int field, int axis, int *src,
                       double *fac, int n);
 
+/* Diagnostics: per-kernel device time measured live with CUDA events on the context's
+ * stream.  Runs `nsteps` exec_ steps (the same work as qas_run, launched eagerly) with an
+ * event pair around every kernel launch and returns, per kernel, the number of launches and
+ * the summed durations.  *count receives the number of entries written (<= max_entries). */
+typedef struct {
+  char name[32];
+  long long launches;
+  double total_ms;
+} qas_kernel_time;
+qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, qas_kernel_time *out,
+                           int max_entries, int *count);
+
+/* Tuning options (defaults are the measured best on B200).
+ *   QAS_OPT_FUSED_SWEEP: 0 = reconstruction and Riemann flux of each direction in two
+ *   kernels with the face states in HBM (default); 1 = one fused sweep kernel.
+ * Both forms give bit-identical results. */
+#define QAS_OPT_FUSED_SWEEP 1
+qas_status qas_set_option(qas_ctx *ctx, int option, int value);
+
 /* Number of kernels this context has launched (eager launches plus kernels inside
  * replayed graphs), for launch accounting. */
 qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);

@@ -69,6 +69,15 @@ struct qas_ctx {
   long long launches = 0;
   bool capturing = false;
   qas_status latched = QAS_OK;
+  // face sweep form: two kernels with the face states in HBM (default, measured faster on
+  // B200: both halves are latency/FP64-bound, the fused kernel spills) or one fused kernel
+  bool fused = false;
+  // live per-kernel timing (qas_profile_run): an event pair around every launch
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_events;
+  std::vector<int> prof_kids;  // kernel id of each recorded pair
+  double prof_ms[32] = {0};
+  long long prof_n[32] = {0};
 };
 
 // ---------------------------------------------------------------------------
@@ -200,12 +209,44 @@ static qas_status build_maps(qas_ctx *c)
 // ---------------------------------------------------------------------------
 namespace {
 
+enum Kid {
+  KID_PRIM, KID_DV, KID_LR, KID_FLUX, KID_EMF, KID_UPDATE, KID_BOUND, KID_BEGIN, KID_VMAX, KID_SETDT,
+  KID_DVEL, KID_ERES, KID_DFLUX, KID_DUPDATE, KID_DBOUND, KID_DCOPY, KID_DSUB, KID_COUNT
+};
+const char *const KID_NAMES[KID_COUNT] = {"k_prim", "k_dv", "k_lr", "k_flux", "k_emf", "k_update", "k_bound",
+                                          "k_begin_step", "k_vmax", "k_setdt", "k_dvel", "k_eres", "k_dflux",
+                                          "k_dupdate", "k_dbound", "k_dcopy", "k_dsub"};
+
+void prof_mark(qas_ctx *c, int kid)
+{
+  const size_t n = c->prof_kids.size();
+  if (c->prof_events.size() < 2 * (n + 1)) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    c->prof_events.push_back(a);
+    c->prof_events.push_back(b);
+  }
+  c->prof_kids.push_back(kid);
+  cudaEventRecord(c->prof_events[2 * n], c->stream);
+}
+void prof_done(qas_ctx *c) { cudaEventRecord(c->prof_events[2 * (c->prof_kids.size() - 1) + 1], c->stream); }
+
+// launch `expr` (one kernel) with optional event timing
+#define QL(c, kid, ...)                    \
+  do {                                     \
+    if ((c)->prof) prof_mark((c), (kid));  \
+    __VA_ARGS__;                           \
+    if ((c)->prof) prof_done((c));         \
+  } while (0)
+
 dim3 cells_grid(const Geo &g) { return dim3((g.nx + BLK - 1) / BLK, g.ny, g.nz); }
 dim3 update_grid(const Geo &g)
 {
   return dim3((g.nx - 2 * GH + 1 + BLK - 1) / BLK, g.dim >= 2 ? g.ny - 2 * GH + 1 : 1,
               g.dim >= 3 ? g.nz - 2 * GH + 1 : 1);
 }
+dim3 shell_grid(const Geo &g) { return dim3((unsigned)((shell_cells(g) + BLK - 1) / BLK)); }
 dim3 interior_grid(const Geo &g)
 {
   return dim3((g.nx - 2 * GH + BLK - 1) / BLK, g.dim >= 2 ? g.ny - 2 * GH : 1, g.dim >= 3 ? g.nz - 2 * GH : 1);
@@ -215,17 +256,33 @@ template <int ODR>
 void launch_lr(qas_ctx *c, int a)
 {
   const dim3 gr = cells_grid(c->geo);
-  if (a == 0) k_lr<ODR, 0><<<gr, BLK, 0, c->stream>>>(c->view);
-  if (a == 1) k_lr<ODR, 1><<<gr, BLK, 0, c->stream>>>(c->view);
-  if (a == 2) k_lr<ODR, 2><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 1) QL(c, KID_LR, k_lr<ODR, 1><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 2) QL(c, KID_LR, k_lr<ODR, 2><<<gr, BLK, 0, c->stream>>>(c->view));
 }
 template <int RMN>
 void launch_flux(qas_ctx *c, int a)
 {
   const dim3 gr = cells_grid(c->geo);
-  if (a == 0) k_flux<RMN, 0><<<gr, BLK, 0, c->stream>>>(c->view);
-  if (a == 1) k_flux<RMN, 1><<<gr, BLK, 0, c->stream>>>(c->view);
-  if (a == 2) k_flux<RMN, 2><<<gr, BLK, 0, c->stream>>>(c->view);
+  if (a == 0) QL(c, KID_FLUX, k_flux<RMN, 0><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 1) QL(c, KID_FLUX, k_flux<RMN, 1><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 2) QL(c, KID_FLUX, k_flux<RMN, 2><<<gr, BLK, 0, c->stream>>>(c->view));
+}
+
+template <int ODR, int RMN>
+void launch_sweep(qas_ctx *c, int a)
+{
+  const Geo &g = c->geo;
+  if (a == 0) {
+    const unsigned nb = (unsigned)((g.nx - 5 + 4 * 31 - 1) / (4 * 31));
+    QL(c, KID_LR, k_sweep_x<ODR, RMN><<<dim3(nb, g.ny, g.nz), 128, 0, c->stream>>>(c->view));
+  } else if (a == 1) {
+    const unsigned ns = (unsigned)((g.ny - 5 + QAS_SWEEP_SEG - 1) / QAS_SWEEP_SEG);
+    QL(c, KID_LR, k_sweep_m<ODR, RMN, 1><<<dim3((g.nx + 127) / 128, ns, g.nz), 128, 0, c->stream>>>(c->view));
+  } else {
+    const unsigned ns = (unsigned)((g.nz - 5 + QAS_SWEEP_SEG - 1) / QAS_SWEEP_SEG);
+    QL(c, KID_LR, k_sweep_m<ODR, RMN, 2><<<dim3((g.nx + 127) / 128, g.ny, ns), 128, 0, c->stream>>>(c->view));
+  }
 }
 
 template <int ODR>
@@ -233,13 +290,23 @@ long long stage_odr(qas_ctx *c, double c0, double c1)
 {
   const Geo &g = c->geo;
   long long nk = 0;
-  k_prim<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+  QL(c, KID_PRIM, k_prim<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
   nk++;
   if (c->scheme.rmn >= 2 && g.dim >= 2) {
-    k_dv<<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+    QL(c, KID_DV, k_dv<<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
     nk++;
   }
   for (int a = 0; a < g.dim; a++) {
+    if (c->fused) {
+      switch (c->scheme.rmn) {
+        case 0: launch_sweep<ODR, 0>(c, a); break;
+        case 1: launch_sweep<ODR, 1>(c, a); break;
+        case 2: launch_sweep<ODR, 2>(c, a); break;
+        default: launch_sweep<ODR, 3>(c, a); break;
+      }
+      nk += 1;
+      continue;
+    }
     launch_lr<ODR>(c, a);
     switch (c->scheme.rmn) {
       case 0: launch_flux<0>(c, a); break;
@@ -250,11 +317,11 @@ long long stage_odr(qas_ctx *c, double c0, double c1)
     nk += 2;
   }
   if (g.dim >= 2) {
-    k_emf<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+    QL(c, KID_EMF, k_emf<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
     nk++;
   }
-  k_update<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c0, c1);
-  k_bound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view);
+  QL(c, KID_UPDATE, k_update<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c0, c1));
+  QL(c, KID_BOUND, k_bound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view));
   nk += 2;
   return nk;
 }
@@ -292,17 +359,17 @@ long long dsptv_odr(qas_ctx *c, int nc, double nu0, double eta0)
   const Geo &g = c->geo;
   const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
   long long nk = 0;
-  k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
-  k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, nc);
+  QL(c, KID_DBOUND, k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
+  QL(c, KID_DCOPY, k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, nc));
   nk += 2;
   for (int rk = 0; rk < c->scheme.rk; rk++) {
     double c0, c1;
     rk_factors(c->scheme.rk, rk, c0, c1);
-    k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
-    k_eres<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, eta0, idx, idy);
-    k_dflux<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, nu0, idx, idy);
-    k_dupdate<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, c0, c1);
-    k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc);
+    QL(c, KID_DVEL, k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
+    QL(c, KID_ERES, k_eres<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, eta0, idx, idy));
+    QL(c, KID_DFLUX, k_dflux<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, nu0, idx, idy));
+    QL(c, KID_DUPDATE, k_dupdate<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, c0, c1));
+    QL(c, KID_DBOUND, k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
     nk += 5;
   }
   return nk;
@@ -324,8 +391,8 @@ long long launch_dissipate(qas_ctx *c, double nu0, double eta0)
   const double dcmax0 = (2 * nu0 >= eta0) ? 2 * nu0 : eta0;
   const double dcmax = dcmax0 > 0.0 ? dcmax0 : 0.0;
   if (!(dcmax > 1e-15)) return 0;
-  k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx, 1.0 / c->grid.dy,
-                                       NSUB_CAP);
+  QL(c, KID_DSUB, k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx, 1.0 / c->grid.dy,
+                                       NSUB_CAP));
   long long nk = 1;
   for (int nc = 0; nc < NSUB_CAP; nc++) nk += launch_dsptv(c, nc, nu0, eta0);
   return nk;
@@ -333,9 +400,9 @@ long long launch_dissipate(qas_ctx *c, double nu0, double eta0)
 
 long long launch_setdt(qas_ctx *c, double cfl, int rule, double dtrec, int nout)
 {
-  k_vmax_reset<<<1, 1, 0, c->stream>>>(c->view);
-  k_vmax<<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view);
-  k_setdt<<<1, 1, 0, c->stream>>>(c->view, cfl, c->dr, rule, dtrec, nout);
+  QL(c, KID_VMAX, k_vmax_reset<<<1, 1, 0, c->stream>>>(c->view));
+  QL(c, KID_VMAX, k_vmax<<<interior_grid(c->geo), BLK, 0, c->stream>>>(c->view));
+  QL(c, KID_SETDT, k_setdt<<<1, 1, 0, c->stream>>>(c->view, cfl, c->dr, rule, dtrec, nout));
   return 3;
 }
 
@@ -343,8 +410,8 @@ long long launch_setdt(qas_ctx *c, double cfl, int rule, double dtrec, int nout)
 long long launch_exec_step(qas_ctx *c, const qas_run_opts &o, int n_after)
 {
   long long nk = 0;
-  k_begin_step<<<1, 1, 0, c->stream>>>(c->view, o.stop_rule == 2 ? 0 : 1);
-  k_bound<<<cells_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  QL(c, KID_BEGIN, k_begin_step<<<1, 1, 0, c->stream>>>(c->view, o.stop_rule == 2 ? 0 : 1));
+  QL(c, KID_BOUND, k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view));
   nk += 2 + launch_ideal(c);
   if (c->grid.dim == 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
   if (o.flg && (n_after % 2 == 0)) nk += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
@@ -510,6 +577,7 @@ qas_status qas_destroy(qas_ctx *c)
   if (!c) return QAS_ERR_INVALID;
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
   if (c->pool) cudaFree(c->pool);
   if (c->d_src) cudaFree(c->d_src);
   if (c->d_fac) cudaFree(c->d_fac);
@@ -589,7 +657,7 @@ qas_status qas_bound(qas_ctx *c)
 {
   if (!c) return QAS_ERR_INVALID;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
-  k_bound<<<cells_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+  k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view);
   c->launches++;
   return check_launch(c);
 }
@@ -756,7 +824,7 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
     k_eres<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, eta0, idx, idy);               \
     k_dflux<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, nu0, idx, idy);               \
     k_dupdate<O><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, c0, c1);                   \
-    k_dbound<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                \
+    k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                \
     break;
       QAS_DST(1)
       QAS_DST(2)
@@ -828,6 +896,78 @@ qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int fie
     fac[i] = m.fac[i];
   }
   return QAS_OK;
+}
+
+qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas_kernel_time *out,
+                           int max_entries, int *count)
+{
+  if (!c || !opts || !out || !count || nsteps <= 0) return QAS_ERR_INVALID;
+  qas_run_opts o = *opts;
+  o.use_graph = 0;
+  o.stop_rule = 0;
+  o.max_steps = 1;
+  qas_status s;
+  // make sure the loop is initialised (setdt(1)) and the stop flag is clear
+  if (!c->run_initialised) {
+    qas_run_opts o0 = o;
+    o0.max_steps = 1;
+    if ((s = qas_run(c, &o0, nullptr)) != QAS_OK) return s;
+  }
+  if ((s = read_ctl(c)) != QAS_OK) return s;
+  c->h_ctl->done = 0;
+  c->h_ctl->nmax = INT_MAX;
+  if ((s = write_ctl(c)) != QAS_OK) return s;
+  for (int k = 0; k < KID_COUNT; k++) {
+    c->prof_ms[k] = 0.0;
+    c->prof_n[k] = 0;
+  }
+  int n_host = c->h_ctl->n;
+  c->prof = true;
+  for (int st = 0; st < nsteps; st++) {
+    c->prof_kids.clear();
+    c->launches += launch_exec_step(c, o, n_host + 1);
+    n_host++;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      c->prof = false;
+      return cuda_fail(e, "profile step");
+    }
+    for (size_t q = 0; q < c->prof_kids.size(); q++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, c->prof_events[2 * q], c->prof_events[2 * q + 1]);
+      c->prof_ms[c->prof_kids[q]] += ms;
+      c->prof_n[c->prof_kids[q]] += 1;
+    }
+  }
+  c->prof = false;
+  c->prof_kids.clear();
+  if ((s = check_launch(c)) != QAS_OK) return s;
+  int w = 0;
+  for (int k = 0; k < KID_COUNT && w < max_entries; k++) {
+    if (!c->prof_n[k]) continue;
+    snprintf(out[w].name, sizeof(out[w].name), "%s", KID_NAMES[k]);
+    out[w].launches = c->prof_n[k];
+    out[w].total_ms = c->prof_ms[k];
+    w++;
+  }
+  *count = w;
+  return read_ctl(c);
+}
+
+qas_status qas_set_option(qas_ctx *c, int option, int value)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (option == QAS_OPT_FUSED_SWEEP) {
+    const bool f = value != 0;
+    if (f != c->fused && c->graph) {  // the captured graph holds the other form
+      cudaStreamSynchronize(c->stream);
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+    c->fused = f;
+    return QAS_OK;
+  }
+  return QAS_ERR_INVALID;
 }
 
 qas_status qas_kernel_launches(const qas_ctx *c, long long *count)

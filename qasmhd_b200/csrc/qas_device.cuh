@@ -267,6 +267,120 @@ __device__ __forceinline__ void face_states(const double q[7][5], double bn, dou
 }
 
 // ---------------------------------------------------------------------------
+// Same reconstruction with the stencil read per characteristic group instead
+// of held in registers: {0,1,2} need ro,vn,bt,bu,pr; {3,4} need vt,bt; {5,6}
+// need vu,bu.  Outputs are accumulated in the reference's term order.
+// `P` is a functor P(v, m) returning primitive v at stencil point m.
+// ---------------------------------------------------------------------------
+template <int ODR, class Stencil>
+__device__ __forceinline__ void face_states_grouped(const Stencil &P, double bn, double gam, double vl[7],
+                                                    double vr[7])
+{
+  const double ro = P(0, 2), vn = P(1, 2), vt = P(2, 2), vu = P(3, 2);
+  const double by = P(4, 2), bz = P(5, 2), pr = P(6, 2);
+  const bool fast = (ro * (vn * vn + vt * vt + vu * vu) > gam * pr);
+  double iro = 1.0 / ro;
+  double cs2 = gam * pr * iro;
+  double ca2 = bn * bn * iro;
+  double ct2 = (by * by + bz * bz) * iro;
+  double cb2 = cs2 + ca2 + ct2;
+  double cf2 = 0.5 * (cb2 + sqrt(fabs(cb2 * cb2 - 4.0 * cs2 * ca2)));
+  double sro = sqrt(ro);
+  double isroh = 0.5 / sro;
+  double icf2 = 1.0 / cf2;
+  double byh = 0.5 * by, bzh = 0.5 * bz;
+  double rcf = 0.0, icf2h = 0.0, ircfh = 0.0;
+  if (fast) {
+    double cf = sqrt(cf2);
+    rcf = ro * cf;
+    icf2h = 0.5 * icf2;
+    ircfh = 0.5 / rcf;
+  }
+  const double nrcf = -rcf;
+  bool zvn = true, zvt = true, zvu = true, zbt = true, zbu = true;
+  double wl0, wr0, wl1, wr1, wl2, wr2, wl3, wr3, wl4, wr4, wl5, wr5, wl6, wr6;
+  {  // fast/alfven/entropy group
+    double w0[5], w1[5], w2[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const double r_ = P(0, m), n_ = P(1, m), b_ = P(4, m), c_ = P(5, m), p_ = P(6, m);
+      zvn = zvn && (n_ == 0.0);
+      zbt = zbt && (b_ == 0.0);
+      zbu = zbu && (c_ == 0.0);
+      w0[m] = fast ? (((nrcf * n_ + by * b_) + bz * c_) + p_) : n_;
+      w1[m] = ((cf2 * r_ - by * b_) - bz * c_) - p_;
+      w2[m] = fast ? (((rcf * n_ + by * b_) + bz * c_) + p_) : ((by * b_ + bz * c_) + p_);
+    }
+    nl_lr<ODR>(w0, wl0, wr0);
+    nl_lr<ODR>(w1, wl1, wr1);
+    nl_lr<ODR>(w2, wl2, wr2);
+  }
+  {  // y-Alfven group
+    double w3[5], w4[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const double t_ = P(2, m), b_ = P(4, m);
+      zvt = zvt && (t_ == 0.0);
+      w3[m] = sro * t_ + b_;
+      w4[m] = sro * t_ - b_;
+    }
+    nl_lr<ODR>(w3, wl3, wr3);
+    nl_lr<ODR>(w4, wl4, wr4);
+  }
+  {  // z-Alfven group
+    double w5[5], w6[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const double u_ = P(3, m), c_ = P(5, m);
+      zvu = zvu && (u_ == 0.0);
+      w5[m] = sro * u_ + c_;
+      w6[m] = sro * u_ - c_;
+    }
+    nl_lr<ODR>(w5, wl5, wr5);
+    nl_lr<ODR>(w6, wl6, wr6);
+  }
+  if (fast) {
+    vl[0] = icf2h * wl0 + icf2 * wl1 + icf2h * wl2;
+    vr[0] = icf2h * wr0 + icf2 * wr1 + icf2h * wr2;
+    vl[1] = (-ircfh) * wl0 + ircfh * wl2;
+    vr[1] = (-ircfh) * wr0 + ircfh * wr2;
+    vl[6] = ((((0.5 * wl0 + 0.5 * wl2) - byh * wl3) + byh * wl4) - bzh * wl5) + bzh * wl6;
+    vr[6] = ((((0.5 * wr0 + 0.5 * wr2) - byh * wr3) + byh * wr4) - bzh * wr5) + bzh * wr6;
+  } else {
+    vl[0] = icf2 * wl1 + icf2 * wl2;
+    vr[0] = icf2 * wr1 + icf2 * wr2;
+    vl[1] = wl0;
+    vr[1] = wr0;
+    vl[6] = (((wl2 - byh * wl3) + byh * wl4) - bzh * wl5) + bzh * wl6;
+    vr[6] = (((wr2 - byh * wr3) + byh * wr4) - bzh * wr5) + bzh * wr6;
+  }
+  vl[2] = isroh * wl3 + isroh * wl4;
+  vr[2] = isroh * wr3 + isroh * wr4;
+  vl[3] = isroh * wl5 + isroh * wl6;
+  vr[3] = isroh * wr5 + isroh * wr6;
+  vl[4] = 0.5 * wl3 - 0.5 * wl4;
+  vr[4] = 0.5 * wr3 - 0.5 * wr4;
+  vl[5] = 0.5 * wl5 - 0.5 * wl6;
+  vr[5] = 0.5 * wr5 - 0.5 * wr6;
+  if (zvn) { vl[1] = 0.0; vr[1] = 0.0; }
+  if (zvt) { vl[2] = 0.0; vr[2] = 0.0; }
+  if (zvu) { vl[3] = 0.0; vr[3] = 0.0; }
+  if (zbt) { vl[4] = 0.0; vr[4] = 0.0; }
+  if (zbu) { vl[5] = 0.0; vr[5] = 0.0; }
+  const double eps = 1e-12;
+  if (vl[0] <= eps || vl[6] <= eps) {
+    vl[0] = ro;
+    vl[1] = vn;
+    vl[6] = pr;
+  }
+  if (vr[0] <= eps || vr[6] <= eps) {
+    vr[0] = ro;
+    vr[1] = vn;
+    vr[6] = pr;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Riemann solvers, common/mhd_flux.c.  L/R = (ro,vn,vt,vu,bt,bu,pr),
 // F = (fro,fmn,fmt,fmu,fbt,fbu,fen).
 // ---------------------------------------------------------------------------

@@ -214,7 +214,10 @@ __global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
 __global__ void k_dbound(View v, const DCtl *dc, int nc)
 {
   QAS_DSUB_GUARD();
-  QAS_CELL_INDEX();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= shell_cells(v.g)) return;
+  int i, j, k;
+  shell_cell(v.g, t, i, j, k);
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
 #pragma unroll

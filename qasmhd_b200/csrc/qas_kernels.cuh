@@ -188,8 +188,22 @@ __global__ void k_dv(View v)
 // ---------------------------------------------------------------------------
 // face states of each cell along axis A (mhd_lrstate + mhd_lr_fb)
 // ---------------------------------------------------------------------------
+#ifndef QAS_LR_MINB
+#define QAS_LR_MINB 5
+#endif
+#ifndef QAS_LR_GROUPED
+#define QAS_LR_GROUPED 1
+#endif
+
+// stencil accessor of k_lr's grouped form: primitive v at point m (0..4) of cell c
+struct LrStencil {
+  const double *p[7];
+  long long c, s;
+  __device__ __forceinline__ double operator()(int v, int m) const { return __ldg(p[v] + c + (m - 2) * s); }
+};
+
 template <int ODR, int A>
-__global__ void __launch_bounds__(128) k_lr(View v)
+__global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
 {
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
@@ -207,6 +221,11 @@ __global__ void __launch_bounds__(128) k_lr(View v)
   const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
   const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
   const double *bnf = v.u[4 + A];
+  double vl[7], vr[7];
+#if QAS_LR_GROUPED
+  const LrStencil st{{v.u[0], vn, vb, vc, cb, ccp, v.pr}, c, s};
+  face_states_grouped<ODR>(st, cn[c], v.gam, vl, vr);
+#else
   double q[7][5];
 #pragma unroll
   for (int m = 0; m < 5; m++) {
@@ -219,8 +238,8 @@ __global__ void __launch_bounds__(128) k_lr(View v)
     q[5][m] = ccp[p];
     q[6][m] = v.pr[p];
   }
-  double vl[7], vr[7];
   face_states<ODR>(q, cn[c], v.gam, vl, vr);
+#endif
 #pragma unroll
   for (int m = 0; m < 7; m++) {
     v.vl[m][c] = vl[m];
@@ -306,6 +325,156 @@ __global__ void __launch_bounds__(128) k_flux(View v)
   v.f[A][4 + B][f] = fbt;
   v.f[A][4 + C][f] = fbu;
   v.f[A][7][f] = F[6];
+}
+
+// ---------------------------------------------------------------------------
+// Fused face sweep along axis A: characteristic face states of every cell and
+// the Riemann flux of every face in one kernel, so the face states never go
+// through HBM.  Along x a warp covers 32 consecutive cells and hands each cell's
+// right-face state to the next lane with a shuffle (31 faces per warp); along y
+// and z each thread marches over a segment of SEG faces and carries the previous
+// cell's state in registers.
+// ---------------------------------------------------------------------------
+#ifndef QAS_SWEEP_MINB
+#define QAS_SWEEP_MINB 4
+#endif
+#ifndef QAS_SWEEP_SEG
+#define QAS_SWEEP_SEG 16
+#endif
+
+template <int ODR, int A>
+__device__ __forceinline__ void cell_states(const View &v, long long c, double vl[7], double vr[7], double ql[2],
+                                            double qr[2])
+{
+  const Geo &g = v.g;
+  const long long s = g.s[A];
+  constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+  const double *vn = A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
+  const double *vb = B == 0 ? v.vx : (B == 1 ? v.vy : v.vz);
+  const double *vc = C == 0 ? v.vx : (C == 1 ? v.vy : v.vz);
+  const double *cn = A == 0 ? v.cx : (A == 1 ? v.cy : v.cz);
+  const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
+  const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
+  const LrStencil st{{v.u[0], vn, vb, vc, cb, ccp, v.pr}, c, s};
+  face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
+  if (g.dim >= 2) {
+    const double *bnf = v.u[4 + A];
+    const double bfl = __ldg(bnf + c + s), bfr = __ldg(bnf + c);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      if (g.dim == 2 && ((A == 0 && t == 1) || (A == 1 && t == 0))) continue;
+      const double *vt = t == 0 ? vb : vc;
+      const double *bt = t == 0 ? cb : ccp;
+      double prod[5], vts[5];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        const long long p = c + (m - 2) * s;
+        prod[m] = __ldg(bt + p) * __ldg(vn + p);
+        vts[m] = __ldg(vt + p);
+      }
+      double fl0, fr0, fl1, fr1;
+      lin_lr<ODR>(prod, fl0, fr0);
+      lin_lr<ODR>(vts, fl1, fr1);
+      ql[t] = fl0 - bfl * fl1;
+      qr[t] = fr0 - bfr * fr1;
+    }
+  }
+}
+
+// flux at face f from the left cell's right-face state L/QL and this cell's left-face state R/QR
+template <int RMN, int A>
+__device__ __forceinline__ void face_flux(const View &v, long long f, const double L[7], const double R[7],
+                                          const double QL[2], const double QR[2])
+{
+  const Geo &g = v.g;
+  const long long s = g.s[A];
+  constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+  double F[7];
+  const double bnf = __ldg(v.u[4 + A] + f);
+  const double bn = 0.5 * (bnf + bnf);
+  double dv0 = 0.0, dv1 = 0.0;
+  if (RMN >= 2) {
+    const double *vn = A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
+    dv0 = __ldg(vn + f) - __ldg(vn + f - s);
+    if (g.dim == 2) {
+      const double *dt = v.dv[A == 0 ? 1 : 0];
+      dv1 = qmin(__ldg(dt + f - s), __ldg(dt + f));
+    } else if (g.dim == 3) {
+      const double *d1 = v.dv[B], *d2 = v.dv[C];
+      dv1 = qmin(qmin(__ldg(d1 + f - s), __ldg(d1 + f)), qmin(__ldg(d2 + f - s), __ldg(d2 + f)));
+    }
+  }
+  riemann<RMN>(L, R, bn, v.gam, dv0, dv1, F);
+  v.f[A][0][f] = F[0];
+  v.f[A][1 + A][f] = F[1];
+  v.f[A][1 + B][f] = F[2];
+  v.f[A][1 + C][f] = F[3];
+  double fbt = F[4], fbu = F[5];
+  if (g.dim >= 2) {
+    if (g.dim == 3 || A == 0) {
+      const double fc0 = 0.5 * (QL[0] + QR[0]);
+      v.fc[A][0][f] = fc0;
+      fbt -= fc0;
+    }
+    if (g.dim == 3 || A == 1) {
+      const double fc1 = 0.5 * (QL[1] + QR[1]);
+      v.fc[A][1][f] = fc1;
+      fbu -= fc1;
+    }
+  }
+  v.f[A][4 + B][f] = fbt;
+  v.f[A][4 + C][f] = fbu;
+  v.f[A][7][f] = F[6];
+}
+
+// x sweep: 4 warps per block, 31 faces per warp
+template <int ODR, int RMN>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB) k_sweep_x(View v)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int f0 = 2 + (blockIdx.x * 4 + wid) * 31;  // cell of lane 0
+  const int i = f0 + lane;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const bool have_cell = i >= 2 && i < g.nx - 2;
+  double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+  const long long c = cidx(g, i < g.nx ? i : g.nx - 1, j, k);
+  if (have_cell) cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
+  double L[7], QL[2];
+#pragma unroll
+  for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
+  QL[0] = __shfl_up_sync(0xffffffffu, ql[0], 1);
+  QL[1] = __shfl_up_sync(0xffffffffu, ql[1], 1);
+  if (lane >= 1 && i >= 3 && i < g.nx - 2) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
+}
+
+// y / z sweep: each thread marches over SEG faces along A, threads along x
+template <int ODR, int RMN, int A>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB) k_sweep_m(View v)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nx) return;
+  const int n = g.n[A];
+  const int p0 = 3 + (A == 1 ? blockIdx.y : blockIdx.z) * QAS_SWEEP_SEG;
+  const int other = A == 1 ? blockIdx.z : blockIdx.y;  // k for the y sweep, j for the z sweep
+  const int p1 = min(p0 + QAS_SWEEP_SEG, n - 2);
+  const long long s = g.s[A];
+  long long c = A == 1 ? cidx(g, i, p0 - 1, other) : cidx(g, i, other, p0 - 1);
+  double L[7], QL[2] = {0.0, 0.0}, tmp[7], tq[2] = {0.0, 0.0};
+  cell_states<ODR, A>(v, c, L, tmp, QL, tq);
+  for (int p = p0; p < p1; p++) {
+    c += s;
+    double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+    cell_states<ODR, A>(v, c, vl, vr, ql, qr);
+    face_flux<RMN, A>(v, c, L, vr, QL, qr);
+#pragma unroll
+    for (int m = 0; m < 7; m++) L[m] = vl[m];
+    QL[0] = ql[0];
+    QL[1] = ql[1];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -460,12 +629,60 @@ __global__ void k_update(View v, double c0, double c1)
 }
 
 // ---------------------------------------------------------------------------
-// ghost fill of the state (bound())
+// ghost fill of the state (bound()), launched over the ghost shell only: the
+// cells with an index in [0,GH) or [n-GH,n) along some active axis
 // ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ long long shell_cells(const Geo &g)
+{
+  const long long ix = g.nx - 2 * GH;
+  if (g.dim == 1) return 2 * GH;
+  if (g.dim == 2) return (long long)g.nx * g.ny - ix * (g.ny - 2 * GH);
+  return (long long)g.nx * g.ny * g.nz - ix * (g.ny - 2 * GH) * (g.nz - 2 * GH);
+}
+
+__device__ __forceinline__ void shell_cell(const Geo &g, long long t, int &i, int &j, int &k)
+{
+  k = 0;
+  j = 0;
+  if (g.dim == 1) {
+    i = t < GH ? (int)t : g.nx - 2 * GH + (int)t;
+    return;
+  }
+  if (g.dim == 3) {
+    const long long plane = (long long)g.nx * g.ny;
+    if (t < 2 * GH * plane) {
+      const int kid = (int)(t / plane);
+      k = kid < GH ? kid : g.nz - 2 * GH + kid;
+      const long long r = t - kid * plane;
+      j = (int)(r / g.nx);
+      i = (int)(r - (long long)j * g.nx);
+      return;
+    }
+    t -= 2 * GH * plane;
+    const long long s2 = plane - (long long)(g.nx - 2 * GH) * (g.ny - 2 * GH);
+    const int kk = (int)(t / s2);
+    k = GH + kk;
+    t -= kk * s2;
+  }
+  if (t < 2 * GH * (long long)g.nx) {
+    const int jid = (int)(t / g.nx);
+    j = jid < GH ? jid : g.ny - 2 * GH + jid;
+    i = (int)(t - (long long)jid * g.nx);
+    return;
+  }
+  t -= 2 * GH * (long long)g.nx;
+  j = GH + (int)(t / (2 * GH));
+  const int col = (int)(t % (2 * GH));
+  i = col < GH ? col : g.nx - 2 * GH + col;
+}
+
 __global__ void k_bound(View v)
 {
   if (v.ctl->done) return;
-  QAS_CELL_INDEX();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= shell_cells(v.g)) return;
+  int i, j, k;
+  shell_cell(v.g, t, i, j, k);
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
 #pragma unroll

@@ -31,8 +31,9 @@ EXPORTS = (
     "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
     "qas_run", "qas_run_reset", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
-    "qas_kernel_launches", "qas_bc_map",
+    "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option",
 )
+QAS_OPT_FUSED_SWEEP = 1
 
 
 class QasError(RuntimeError):
@@ -64,6 +65,10 @@ class RunOpts(ctypes.Structure):
     _fields_ = [("max_steps", ctypes.c_int), ("flg", ctypes.c_int), ("stop_rule", ctypes.c_int),
                 ("cfl", ctypes.c_double), ("dtrec", ctypes.c_double), ("nout", ctypes.c_int),
                 ("use_graph", ctypes.c_int), ("nu0", ctypes.c_double), ("eta0", ctypes.c_double)]
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double)]
 
 
 class RunInfo(ctypes.Structure):
@@ -111,6 +116,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_max_divb.argtypes = [vp, dp]
     lib.qas_sync.argtypes = [vp]
     lib.qas_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.qas_profile_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.c_int, ctypes.POINTER(KernelTime),
+                                    ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.qas_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -229,6 +237,18 @@ class Context:
         info = RunInfo()
         _check(self.lib.qas_run(self.h, ctypes.byref(o), ctypes.byref(info)), "qas_run")
         return info
+
+    def profile(self, nsteps: int, flg: int = 1, cfl: float = 0.4, nu0: float = 0.0, eta0: float = 0.0) -> dict:
+        """Per-kernel {name: (launches, total_ms)} over nsteps eager exec_ steps (CUDA events)."""
+        o = RunOpts(1, int(flg), 0, float(cfl), 1.0, 1, 0, float(nu0), float(eta0))
+        out = (KernelTime * 32)()
+        cnt = ctypes.c_int()
+        _check(self.lib.qas_profile_run(self.h, ctypes.byref(o), int(nsteps), out, 32, ctypes.byref(cnt)),
+               "qas_profile_run")
+        return {out[i].name.decode(): (int(out[i].launches), float(out[i].total_ms)) for i in range(cnt.value)}
+
+    def set_option(self, option: int, value: int) -> None:
+        _check(self.lib.qas_set_option(self.h, int(option), int(value)), "qas_set_option")
 
     def run_reset(self) -> None:
         _check(self.lib.qas_run_reset(self.h), "qas_run_reset")

@@ -175,3 +175,25 @@ def test_kh_256_determinism_and_divb():
     assert np.isfinite(outs[0]).all()
     assert_bitwise(outs[0], outs[1], "repeat")
     assert d < 1e-10, d
+
+
+@pytest.mark.parametrize("dim,rmn", [(1, 1), (2, 1), (2, 3), (3, 0), (3, 3)])
+def test_fused_sweep_form(restatement, dim, rmn):
+    p = {1: lambda: P.brio_wu(96, rmn=rmn), 2: lambda: P.orszag_tang(48, rmn=rmn),
+         3: lambda: P.kelvin_helmholtz(3, 12, mach=0.3, rmn=rmn)}[dim]()
+    a = restatement.run(p, 3, mode=R.MODE_RUN)
+    with L.Context.from_problem(p) as ctx:
+        ctx.set_option(L.QAS_OPT_FUSED_SWEEP, 1)
+        ctx.upload(p.state)
+        ctx.run(max_steps=3, flg=p.flg, stop_rule=0, cfl=p.cfl)
+        out = ctx.download(p.state.shape)
+    assert_bitwise(out, a["state"], f"fused dim{dim} rmn{rmn}")
+
+
+def test_profile_run_reports_kernels():
+    p = P.orszag_tang(64)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        prof = ctx.profile(2)
+    assert prof["k_lr"][0] == 2 * 3 * 2 and prof["k_flux"][0] == 2 * 3 * 2
+    assert all(ms > 0 for _, ms in prof.values())
