@@ -184,6 +184,17 @@ qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, q
 #define QAS_OPT_FUSED_SWEEP 1
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
+/* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel
+ * ("k_prim", "k_dv", "k_lr", "k_flux", "k_emf", "k_update") or of all of them ("all"). */
+qas_status qas_set_tile(qas_ctx *ctx, const char *kernel, int tx, int ty, int tz);
+qas_status qas_get_tile(const qas_ctx *ctx, const char *kernel, int *tx, int *ty, int *tz);
+
+/* Autotuner: for each cell kernel, time the candidate tiles over `trial_steps` exec_ steps
+ * with CUDA events and keep the fastest.  The state, dt, time and step counter are restored
+ * afterwards (results do not depend on the tile: every tile gives bit-identical states).
+ * Choices are cached per (dim, ODR, RMN, grid-size bucket) for the life of the process. */
+qas_status qas_autotune(qas_ctx *ctx, int trial_steps);
+
 /* Number of kernels this context has launched (eager launches plus kernels inside
  * replayed graphs), for launch accounting. */
 qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -69,6 +70,8 @@ struct qas_ctx {
   long long launches = 0;
   bool capturing = false;
   qas_status latched = QAS_OK;
+  // thread-block tile (x,y,z extents, 128 threads) of every cell kernel, by kernel id
+  dim3 tile[32];
   // face sweep form: two kernels with the face states in HBM (default, measured faster on
   // B200: both halves are latency/FP64-bound, the fused kernel spills) or one fused kernel
   bool fused = false;
@@ -240,11 +243,14 @@ void prof_done(qas_ctx *c) { cudaEventRecord(c->prof_events[2 * (c->prof_kids.si
     if ((c)->prof) prof_done((c));         \
   } while (0)
 
-dim3 cells_grid(const Geo &g) { return dim3((g.nx + BLK - 1) / BLK, g.ny, g.nz); }
-dim3 update_grid(const Geo &g)
+dim3 cells_grid(const Geo &g, dim3 t = dim3(BLK, 1, 1))
 {
-  return dim3((g.nx - 2 * GH + 1 + BLK - 1) / BLK, g.dim >= 2 ? g.ny - 2 * GH + 1 : 1,
-              g.dim >= 3 ? g.nz - 2 * GH + 1 : 1);
+  return dim3((g.nx + t.x - 1) / t.x, (g.ny + t.y - 1) / t.y, (g.nz + t.z - 1) / t.z);
+}
+dim3 update_grid(const Geo &g, dim3 t = dim3(BLK, 1, 1))
+{
+  const int ny = g.dim >= 2 ? g.ny - 2 * GH + 1 : 1, nz = g.dim >= 3 ? g.nz - 2 * GH + 1 : 1;
+  return dim3((g.nx - 2 * GH + 1 + t.x - 1) / t.x, (ny + t.y - 1) / t.y, (nz + t.z - 1) / t.z);
 }
 dim3 shell_grid(const Geo &g) { return dim3((unsigned)((shell_cells(g) + BLK - 1) / BLK)); }
 dim3 interior_grid(const Geo &g)
@@ -255,18 +261,16 @@ dim3 interior_grid(const Geo &g)
 template <int ODR>
 void launch_lr(qas_ctx *c, int a)
 {
-  const dim3 gr = cells_grid(c->geo);
-  if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<gr, BLK, 0, c->stream>>>(c->view));
-  if (a == 1) QL(c, KID_LR, k_lr<ODR, 1><<<gr, BLK, 0, c->stream>>>(c->view));
-  if (a == 2) QL(c, KID_LR, k_lr<ODR, 2><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
+  if (a == 1) QL(c, KID_LR, k_lr<ODR, 1><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
+  if (a == 2) QL(c, KID_LR, k_lr<ODR, 2><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
 }
 template <int RMN>
 void launch_flux(qas_ctx *c, int a)
 {
-  const dim3 gr = cells_grid(c->geo);
-  if (a == 0) QL(c, KID_FLUX, k_flux<RMN, 0><<<gr, BLK, 0, c->stream>>>(c->view));
-  if (a == 1) QL(c, KID_FLUX, k_flux<RMN, 1><<<gr, BLK, 0, c->stream>>>(c->view));
-  if (a == 2) QL(c, KID_FLUX, k_flux<RMN, 2><<<gr, BLK, 0, c->stream>>>(c->view));
+  if (a == 0) QL(c, KID_FLUX, k_flux<RMN, 0><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+  if (a == 1) QL(c, KID_FLUX, k_flux<RMN, 1><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+  if (a == 2) QL(c, KID_FLUX, k_flux<RMN, 2><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
 }
 
 template <int ODR, int RMN>
@@ -290,10 +294,10 @@ long long stage_odr(qas_ctx *c, double c0, double c1)
 {
   const Geo &g = c->geo;
   long long nk = 0;
-  QL(c, KID_PRIM, k_prim<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
+  QL(c, KID_PRIM, k_prim<ODR><<<cells_grid(g, c->tile[KID_PRIM]), c->tile[KID_PRIM], 0, c->stream>>>(c->view));
   nk++;
   if (c->scheme.rmn >= 2 && g.dim >= 2) {
-    QL(c, KID_DV, k_dv<<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
+    QL(c, KID_DV, k_dv<<<cells_grid(g, c->tile[KID_DV]), c->tile[KID_DV], 0, c->stream>>>(c->view));
     nk++;
   }
   for (int a = 0; a < g.dim; a++) {
@@ -317,10 +321,10 @@ long long stage_odr(qas_ctx *c, double c0, double c1)
     nk += 2;
   }
   if (g.dim >= 2) {
-    QL(c, KID_EMF, k_emf<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view));
+    QL(c, KID_EMF, k_emf<ODR><<<cells_grid(g, c->tile[KID_EMF]), c->tile[KID_EMF], 0, c->stream>>>(c->view));
     nk++;
   }
-  QL(c, KID_UPDATE, k_update<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c0, c1));
+  QL(c, KID_UPDATE, k_update<ODR><<<update_grid(g, c->tile[KID_UPDATE]), c->tile[KID_UPDATE], 0, c->stream>>>(c->view, c0, c1));
   QL(c, KID_BOUND, k_bound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view));
   nk += 2;
   return nk;
@@ -515,6 +519,10 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
     return s;
   };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(QAS_ERR_CUDA);
+  {
+    const dim3 t = gr.dim == 1 ? dim3(128, 1, 1) : (gr.dim == 2 ? dim3(32, 4, 1) : dim3(32, 2, 2));
+    for (int q = 0; q < 32; q++) c->tile[q] = t;
+  }
   if ((st = build_maps(c)) != QAS_OK) return fail(st);
 
   // one pool for every field array, 256-byte aligned
@@ -968,6 +976,151 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
     return QAS_OK;
   }
   return QAS_ERR_INVALID;
+}
+
+static int tile_kid(const char *k)
+{
+  if (!k) return -2;
+  const int kids[6] = {KID_PRIM, KID_DV, KID_LR, KID_FLUX, KID_EMF, KID_UPDATE};
+  if (!strcmp(k, "all")) return -1;
+  for (int q = 0; q < 6; q++)
+    if (!strcmp(k, KID_NAMES[kids[q]])) return kids[q];
+  return -2;
+}
+
+static void drop_graph(qas_ctx *c)
+{
+  if (c->graph) {
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+}
+
+qas_status qas_set_tile(qas_ctx *c, const char *kernel, int tx, int ty, int tz)
+{
+  if (!c) return QAS_ERR_INVALID;
+  const int kid = tile_kid(kernel);
+  if (kid == -2 || tx < 32 || tx % 32 || ty < 1 || tz < 1 || tx * ty * tz > 128) return QAS_ERR_INVALID;
+  if (c->grid.dim < 2 && ty != 1) return QAS_ERR_INVALID;
+  if (c->grid.dim < 3 && tz != 1) return QAS_ERR_INVALID;
+  drop_graph(c);
+  const dim3 t(tx, ty, tz);
+  if (kid == -1) {
+    for (int q = 0; q < 32; q++) c->tile[q] = t;
+  } else {
+    c->tile[kid] = t;
+  }
+  return QAS_OK;
+}
+
+qas_status qas_get_tile(const qas_ctx *c, const char *kernel, int *tx, int *ty, int *tz)
+{
+  if (!c || !tx || !ty || !tz) return QAS_ERR_INVALID;
+  const int kid = tile_kid(kernel);
+  if (kid < 0) return QAS_ERR_INVALID;
+  *tx = c->tile[kid].x;
+  *ty = c->tile[kid].y;
+  *tz = c->tile[kid].z;
+  return QAS_OK;
+}
+
+namespace {
+struct TuneKey {
+  int dim, odr, rmn, bucket;
+  bool operator==(const TuneKey &o) const
+  {
+    return dim == o.dim && odr == o.odr && rmn == o.rmn && bucket == o.bucket;
+  }
+};
+struct TuneEntry {
+  TuneKey key;
+  dim3 tiles[6];
+};
+std::vector<TuneEntry> g_tune_cache;
+std::mutex g_tune_mu;
+}  // namespace
+
+qas_status qas_autotune(qas_ctx *c, int trial_steps)
+{
+  if (!c || trial_steps <= 0) return QAS_ERR_INVALID;
+  const int kids[6] = {KID_PRIM, KID_DV, KID_LR, KID_FLUX, KID_EMF, KID_UPDATE};
+  int bucket = 0;
+  for (long long n = c->geo.nd; n > 4096; n >>= 2) bucket++;
+  const TuneKey key{c->grid.dim, c->scheme.odr, c->scheme.rmn, bucket};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneEntry &e : g_tune_cache)
+      if (e.key == key) {
+        drop_graph(c);
+        for (int q = 0; q < 6; q++) c->tile[kids[q]] = e.tiles[q];
+        return QAS_OK;
+      }
+  }
+  std::vector<dim3> cands;
+  if (c->grid.dim == 1) {
+    cands = {dim3(128, 1, 1), dim3(64, 1, 1), dim3(32, 1, 1)};
+  } else if (c->grid.dim == 2) {
+    cands = {dim3(128, 1, 1), dim3(64, 2, 1), dim3(32, 4, 1), dim3(32, 2, 1)};
+  } else {
+    cands = {dim3(128, 1, 1), dim3(64, 2, 1), dim3(32, 4, 1), dim3(32, 2, 2), dim3(32, 1, 4), dim3(64, 1, 2)};
+  }
+  // save the state and the loop counters
+  qas_status s;
+  if ((s = read_ctl(c)) != QAS_OK) return s;
+  const Ctl saved_ctl = *c->h_ctl;
+  const bool saved_init = c->run_initialised;
+  const size_t bytes = (size_t)c->geo.nd * sizeof(double);
+  double *backup = nullptr;
+  QAS_CUDA(cudaMalloc(&backup, 8 * bytes));
+  for (int m = 0; m < 8; m++)
+    cudaMemcpyAsync(backup + (size_t)m * c->geo.nd, c->view.u[m], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  drop_graph(c);
+  qas_run_opts o{};
+  o.flg = 1;
+  o.cfl = 0.4;
+  o.dtrec = 1.0;
+  o.nout = 1;
+  double best_ms[6];
+  dim3 best[6];
+  for (int q = 0; q < 6; q++) {
+    best_ms[q] = 1e300;
+    best[q] = c->tile[kids[q]];
+  }
+  qas_kernel_time kt[32];
+  int cnt = 0;
+  for (const dim3 &t : cands) {
+    for (int q = 0; q < 6; q++) c->tile[kids[q]] = t;
+    // restore the state before each trial so every candidate sees the same work
+    for (int m = 0; m < 8; m++)
+      cudaMemcpyAsync(c->view.u[m], backup + (size_t)m * c->geo.nd, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    *c->h_ctl = saved_ctl;
+    c->h_ctl->done = 0;
+    if ((s = write_ctl(c)) != QAS_OK) break;
+    c->run_initialised = true;
+    if ((s = qas_profile_run(c, &o, trial_steps, kt, 32, &cnt)) != QAS_OK) break;
+    for (int e = 0; e < cnt; e++)
+      for (int q = 0; q < 6; q++)
+        if (!strcmp(kt[e].name, KID_NAMES[kids[q]]) && kt[e].total_ms < best_ms[q]) {
+          best_ms[q] = kt[e].total_ms;
+          best[q] = t;
+        }
+  }
+  for (int q = 0; q < 6; q++) c->tile[kids[q]] = best[q];
+  for (int m = 0; m < 8; m++)
+    cudaMemcpyAsync(c->view.u[m], backup + (size_t)m * c->geo.nd, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  *c->h_ctl = saved_ctl;
+  qas_status s2 = write_ctl(c);
+  c->run_initialised = saved_init;
+  cudaFree(backup);
+  if (s != QAS_OK) return s;
+  if (s2 != QAS_OK) return s2;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  TuneEntry e;
+  e.key = key;
+  for (int q = 0; q < 6; q++) e.tiles[q] = best[q];
+  g_tune_cache.push_back(e);
+  return QAS_OK;
 }
 
 qas_status qas_kernel_launches(const qas_ctx *c, long long *count)

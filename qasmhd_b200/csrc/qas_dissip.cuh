@@ -185,8 +185,8 @@ __global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
   QAS_DSUB_GUARD();
   const Geo &g = v.g;
   const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = GH + blockIdx.y;
-  if (i > g.nx - GH) return;
+  const int j = GH + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > g.nx - GH || j > g.ny - GH || blockIdx.z * blockDim.z + threadIdx.z > 0) return;
   const long long c = cidx(g, i, j, 0);
   const long long sy = g.s[1];
   const double dtdx = dc->sdtd[0], dtdy = dc->sdtd[1];

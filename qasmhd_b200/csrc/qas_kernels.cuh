@@ -97,11 +97,12 @@ __device__ __forceinline__ void gather_src(const View &v, int G, int f, int i, i
   }
 }
 
-#define QAS_CELL_INDEX()                                   \
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;     \
-  const int j = blockIdx.y;                                \
-  const int k = blockIdx.z;                                \
-  if (i >= v.g.nx) return;
+// cell of this thread: blocks tile the grid in x, y and z (tile = blockDim)
+#define QAS_CELL_INDEX()                                              \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;                \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;                \
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;                \
+  if (i >= v.g.nx || j >= v.g.ny || k >= v.g.nz) return;
 
 // ---------------------------------------------------------------------------
 // primitives + cell-centre B (prmtv, bcell/bb2cc + bound(cx,cy,cz))
@@ -569,9 +570,13 @@ __global__ void k_update(View v, double c0, double c1)
   if (v.ctl->done) return;
   const Geo &g = v.g;
   const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
-  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
+  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z * blockDim.z + threadIdx.z;
   if (i > g.nx - GH) return;
+  if (g.dim >= 2 && j > g.ny - GH) return;
+  if (g.dim >= 3 && k > g.nz - GH) return;
+  if (g.dim < 2 && j > 0) return;
+  if (g.dim < 3 && k > 0) return;
   const long long c = cidx(g, i, j, k);
   const double dtdx = v.ctl->dtd[0], dtdy = v.ctl->dtd[1], dtdz = v.ctl->dtd[2];
   const bool ci = i < g.nx - GH;

@@ -31,7 +31,8 @@ EXPORTS = (
     "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
     "qas_run", "qas_run_reset", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
-    "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option",
+    "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
+    "qas_get_tile", "qas_autotune",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -119,6 +120,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_profile_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.c_int, ctypes.POINTER(KernelTime),
                                     ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.qas_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qas_set_tile.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qas_get_tile.argtypes = [vp, ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 3
+    lib.qas_autotune.argtypes = [vp, ctypes.c_int]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -249,6 +253,18 @@ class Context:
 
     def set_option(self, option: int, value: int) -> None:
         _check(self.lib.qas_set_option(self.h, int(option), int(value)), "qas_set_option")
+
+    def set_tile(self, kernel: str, tx: int, ty: int = 1, tz: int = 1) -> None:
+        _check(self.lib.qas_set_tile(self.h, kernel.encode(), tx, ty, tz), "qas_set_tile")
+
+    def get_tile(self, kernel: str):
+        t = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
+        _check(self.lib.qas_get_tile(self.h, kernel.encode(), *[ctypes.byref(x) for x in t]), "qas_get_tile")
+        return tuple(x.value for x in t)
+
+    def autotune(self, trial_steps: int = 2) -> dict:
+        _check(self.lib.qas_autotune(self.h, int(trial_steps)), "qas_autotune")
+        return {k: self.get_tile(k) for k in ("k_prim", "k_dv", "k_lr", "k_flux", "k_emf", "k_update")}
 
     def run_reset(self) -> None:
         _check(self.lib.qas_run_reset(self.h), "qas_run_reset")

@@ -197,3 +197,27 @@ def test_profile_run_reports_kernels():
         prof = ctx.profile(2)
     assert prof["k_lr"][0] == 2 * 3 * 2 and prof["k_flux"][0] == 2 * 3 * 2
     assert all(ms > 0 for _, ms in prof.values())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_tiles_bit_identical(restatement, dim):
+    p = P.orszag_tang(40) if dim == 2 else P.kelvin_helmholtz(3, 12, mach=0.3)
+    a = restatement.run(p, 2, mode=R.MODE_RUN)
+    tiles = [(128, 1, 1), (64, 2, 1), (32, 4, 1)] + ([(32, 2, 2), (32, 1, 4)] if dim == 3 else [(32, 2, 1)])
+    for t in tiles:
+        with L.Context.from_problem(p) as ctx:
+            ctx.set_tile("all", *t)
+            ctx.upload(p.state)
+            ctx.run(max_steps=2, flg=1, stop_rule=0, cfl=p.cfl)
+            assert_bitwise(ctx.download(p.state.shape), a["state"], f"tile {t}")
+
+
+def test_autotune_restores_state(restatement):
+    p = P.orszag_tang(64)
+    a = restatement.run(p, 3, mode=R.MODE_RUN)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        tiles = ctx.autotune(1)
+        assert set(tiles) == {"k_prim", "k_dv", "k_lr", "k_flux", "k_emf", "k_update"}
+        ctx.run(max_steps=3, flg=1, stop_rule=0, cfl=p.cfl)
+        assert_bitwise(ctx.download(p.state.shape), a["state"], "after autotune")
