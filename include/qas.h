@@ -199,6 +199,30 @@ qas_status qas_autotune(qas_ctx *ctx, int trial_steps);
  * replayed graphs), for launch accounting. */
 qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);
 
+/* ------------------------------------------------------------------------------------
+ * Batched ensemble: many independent instances stepped by one set of kernel launches per
+ * stage (one graph-captured launch sequence for the whole ensemble).  The reference runs
+ * one simulation per process with a compile-time grid; this entry point has no counterpart
+ * there beyond running many of its exec_() loops.  All instances share dim, ODR and R_K;
+ * grid sizes, gamma, boundary flags, Riemann solver and CUCT flag are per instance.  Each
+ * instance keeps its own dt (setdt every 2nd step), time and step counter.
+ * ------------------------------------------------------------------------------------ */
+typedef struct qas_batch qas_batch;
+qas_status qas_batch_create(qas_batch **batch, int n, const qas_grid *grids, const qas_scheme *schemes,
+                            const qas_bc *bcs, int device);
+qas_status qas_batch_destroy(qas_batch *batch);
+qas_status qas_batch_cells(const qas_batch *batch, int instance, long long *nd);
+/* state of one instance as one contiguous host block of 8*nd doubles (field-major) */
+qas_status qas_batch_upload(qas_batch *batch, int instance, const double *block);
+qas_status qas_batch_download(qas_batch *batch, int instance, double *block);
+/* exec_ loops of every instance; info (n entries, may be NULL) receives each instance's counters */
+qas_status qas_batch_run(qas_batch *batch, const qas_run_opts *opts, qas_run_info *info);
+qas_status qas_batch_set_tile(qas_batch *batch, const char *kernel, int tx, int ty, int tz);
+/* time candidate tiles per kernel over trial_steps steps (state restored) and keep the fastest */
+qas_status qas_batch_autotune(qas_batch *batch, int trial_steps);
+qas_status qas_batch_stream(qas_batch *batch, void **stream);
+qas_status qas_batch_kernel_launches(const qas_batch *batch, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

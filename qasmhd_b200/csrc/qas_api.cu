@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/qas.h"
+#include "qas_batch.cuh"
 #include "qas_dissip.cuh"
 #include "qas_kernels.cuh"
 
@@ -550,6 +551,7 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   v.dx = gr.dx;
   v.dy = gr.dim >= 2 ? gr.dy : 1.0;
   v.dz = gr.dim >= 3 ? gr.dz : 1.0;
+  v.dr = c->dr;
   for (int m = 0; m < 8; m++) v.u[m] = take();
   for (int m = 0; m < 8; m++) v.u0[m] = take();
   v.vx = take(); v.vy = take(); v.vz = take(); v.pr = take();
@@ -1131,3 +1133,5 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 }
 
 }  // extern "C"
+
+#include "qas_batch_api.inc"

@@ -1,0 +1,168 @@
+// qas_batch.cuh -- batched-ensemble kernels: one launch per stage covers every
+// instance of the ensemble.  Blocks are persistent (grid-stride over the block
+// list); a block map gives each block its instance and its block index inside
+// that instance's launch grid, so every block works on one instance with that
+// instance's View (its own sizes, boundary maps, scheme and dt).  The per-cell
+// arithmetic is the single-instance kernels' device bodies.
+#pragma once
+
+#include "qas_kernels.cuh"
+
+namespace qas {
+
+struct BMap {
+  int nblocks;
+  const int2 *blk;   // (instance, local block index) per block
+  const int4 *grid;  // per instance: launch grid in blocks (x, y, z)
+};
+
+#define QAS_BATCH_BLOCKS(map)                                                         \
+  for (int b_ = blockIdx.x; b_ < (map).nblocks; b_ += gridDim.x) {                    \
+    const int2 bi_ = (map).blk[b_];                                                   \
+    const View &v = views[bi_.x];                                                     \
+    if (v.ctl->done) continue;                                                        \
+    const int4 gd_ = (map).grid[bi_.x];                                               \
+    const int bx_ = bi_.y % gd_.x, by_ = (bi_.y / gd_.x) % gd_.y, bz_ = bi_.y / (gd_.x * gd_.y); \
+    const int ti = bx_ * blockDim.x + threadIdx.x;                                    \
+    const int tj = by_ * blockDim.y + threadIdx.y;                                    \
+    const int tk = bz_ * blockDim.z + threadIdx.z;
+
+#define QAS_BATCH_END }
+
+#define QAS_BATCH_CELL_OK (ti < v.g.nx && tj < v.g.ny && tk < v.g.nz)
+
+template <int ODR>
+__global__ void kb_prim(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) prim_body<ODR>(v, ti, tj, tk);
+  QAS_BATCH_END
+}
+
+__global__ void kb_dv(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) dv_body(v, ti, tj, tk);
+  QAS_BATCH_END
+}
+
+template <int ODR, int A>
+__global__ void __launch_bounds__(128, QAS_LR_MINB) kb_lr(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) {
+    const int pos = A == 0 ? ti : (A == 1 ? tj : tk);
+    if (pos >= 2 && pos < v.g.n[A] - 2) lr_body<ODR, A>(v, ti, tj, tk);
+  }
+  QAS_BATCH_END
+}
+
+template <int RMN, int A>
+__global__ void __launch_bounds__(128) kb_flux(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) {
+    const int pos = A == 0 ? ti : (A == 1 ? tj : tk);
+    if (pos >= 3 && pos < v.g.n[A] - 2) flux_body<RMN, A>(v, ti, tj, tk);
+  }
+  QAS_BATCH_END
+}
+
+template <int ODR>
+__global__ void kb_emf(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) emf_body<ODR>(v, ti, tj, tk);
+  QAS_BATCH_END
+}
+
+template <int ODR>
+__global__ void kb_update(const View *__restrict__ views, BMap map, double c0, double c1)
+{
+  QAS_BATCH_BLOCKS(map)
+  int i, j, k;
+  if (update_cell(v.g, ti, tj, tk, i, j, k)) update_body<ODR>(v, i, j, k, c0, c1);
+  QAS_BATCH_END
+}
+
+// ghost shell (1D block index over the shell cells of each instance)
+__global__ void kb_bound(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  (void)tj;
+  (void)tk;
+  if (ti < shell_cells(v.g)) {
+    int i, j, k;
+    shell_cell(v.g, ti, i, j, k);
+    bound_body(v, i, j, k);
+  }
+  QAS_BATCH_END
+}
+
+// u0 = u for all cells of every instance (the copy of ut at the start of ideal)
+__global__ void kb_copy_u0(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) {
+    const long long c = cidx(v.g, ti, tj, tk);
+#pragma unroll
+    for (int m = 0; m < 8; m++) v.u0[m][c] = v.u[m][c];
+  }
+  QAS_BATCH_END
+}
+
+// per-instance control: one thread per instance
+__global__ void kb_begin(const View *__restrict__ views, int n, int check_tim)
+{
+  const int inst = blockIdx.x * blockDim.x + threadIdx.x;
+  if (inst < n) begin_body(views[inst], check_tim);
+}
+__global__ void kb_vmax_reset(const View *__restrict__ views, int n)
+{
+  const int inst = blockIdx.x * blockDim.x + threadIdx.x;
+  if (inst < n && !views[inst].ctl->done)
+    views[inst].ctl->vmax_bits = (unsigned long long)__double_as_longlong(1.0);
+}
+__global__ void kb_setdt(const View *__restrict__ views, int n, double cfl, int rule, double dtrec, int nout)
+{
+  const int inst = blockIdx.x * blockDim.x + threadIdx.x;
+  if (inst < n) setdt_body(views[inst], cfl, views[inst].dr, rule, dtrec, nout);
+}
+
+// per-instance max of |v|+c_f over the interior (1D blocks of 128 threads)
+__global__ void kb_vmax(const View *__restrict__ views, BMap map)
+{
+  __shared__ double red[4];
+  for (int b_ = blockIdx.x; b_ < map.nblocks; b_ += gridDim.x) {
+    const int2 bi = map.blk[b_];
+    const View &v = views[bi.x];
+    if (v.ctl->done) continue;  // uniform over the block
+    const int4 gd = map.grid[bi.x];
+    const int bx = bi.y % gd.x, by = (bi.y / gd.x) % gd.y, bz = bi.y / (gd.x * gd.y);
+    const Geo &g = v.g;
+    const int i = GH + bx * blockDim.x + threadIdx.x;
+    const int j = (g.dim >= 2 ? GH : 0) + by;
+    const int k = (g.dim >= 3 ? GH : 0) + bz;
+    double best = 1.0;
+    if (i < g.nx - GH) {
+      const double vt = vmax_cell(v, i, j, k);
+      if (vt > best) best = vt;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, best, o);
+      best = (other > best) ? other : best;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = red[0];
+      for (int q = 1; q < (int)(blockDim.x >> 5); q++) m = (red[q] > m) ? red[q] : m;
+      atomicMax(&v.ctl->vmax_bits, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace qas

@@ -63,6 +63,7 @@ struct View {
   double *ex, *ey, *ez;
   Ctl *ctl;
   Maps maps;
+  double dr;  // min cell size, the dr of setdt
 };
 
 __device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
@@ -108,10 +109,8 @@ __device__ __forceinline__ void gather_src(const View &v, int G, int f, int i, i
 // primitives + cell-centre B (prmtv, bcell/bb2cc + bound(cx,cy,cz))
 // ---------------------------------------------------------------------------
 template <int ODR>
-__global__ void k_prim(View v)
+__device__ __forceinline__ void prim_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  QAS_CELL_INDEX();
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
   double cx, cy, cz;
@@ -161,14 +160,19 @@ __global__ void k_prim(View v)
                   (g.dim < 3 || (k >= GH && k < g.nz - GH));
   if (interior && !(ro > 0.0 && pr > 0.0 && isfinite(vx) && isfinite(vy) && isfinite(vz))) atomicOr(&v.ctl->err, 1);
 }
+template <int ODR>
+__global__ void k_prim(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  prim_body<ODR>(v, i, j, k);
+}
 
 // ---------------------------------------------------------------------------
 // shock detector dv (mhd2d_solve.cpp:105-125, mhd3d_solve.cpp:138-164)
 // ---------------------------------------------------------------------------
-__global__ void k_dv(View v)
+__device__ __forceinline__ void dv_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  QAS_CELL_INDEX();
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
   const double *vel[3] = {v.vx, v.vy, v.vz};
@@ -184,6 +188,12 @@ __global__ void k_dv(View v)
     const double raw = qmin((p[s + st] - p[s]), (p[s] - p[s - st]));
     v.dv[a][c] = fac * raw;
   }
+}
+__global__ void k_dv(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  dv_body(v, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -204,10 +214,8 @@ struct LrStencil {
 };
 
 template <int ODR, int A>
-__global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
+__device__ __forceinline__ void lr_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  QAS_CELL_INDEX();
   const Geo &g = v.g;
   const int pos = A == 0 ? i : (A == 1 ? j : k);
   const int n = g.n[A];
@@ -269,15 +277,20 @@ __global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
     }
   }
 }
+template <int ODR, int A>
+__global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  lr_body<ODR, A>(v, i, j, k);
+}
 
 // ---------------------------------------------------------------------------
 // Riemann flux per face along axis A (mhd2d_solve.cpp:172-199 and 3D analogues)
 // ---------------------------------------------------------------------------
 template <int RMN, int A>
-__global__ void __launch_bounds__(128) k_flux(View v)
+__device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  QAS_CELL_INDEX();
   const Geo &g = v.g;
   const int pos = A == 0 ? i : (A == 1 ? j : k);
   const int n = g.n[A];
@@ -326,6 +339,13 @@ __global__ void __launch_bounds__(128) k_flux(View v)
   v.f[A][4 + B][f] = fbt;
   v.f[A][4 + C][f] = fbu;
   v.f[A][7][f] = F[6];
+}
+template <int RMN, int A>
+__global__ void __launch_bounds__(128) k_flux(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  flux_body<RMN, A>(v, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -512,10 +532,8 @@ __device__ __forceinline__ double cuct_at(const View &v, const double *va, const
 }
 
 template <int ODR>
-__global__ void k_emf(View v)
+__device__ __forceinline__ void emf_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  QAS_CELL_INDEX();
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
   const long long sx = 1, sy = g.s[1], sz = g.s[2];
@@ -553,6 +571,13 @@ __global__ void k_emf(View v)
     v.ex[c] = ex;
   }
 }
+template <int ODR>
+__global__ void k_emf(View v)
+{
+  if (v.ctl->done) return;
+  QAS_CELL_INDEX();
+  emf_body<ODR>(v, i, j, k);
+}
 
 // ---------------------------------------------------------------------------
 // SSP-RK combine + CT update (mhd_updt1d/2d/3d, mhd_updt2d_ctb/3d_ctb:
@@ -564,19 +589,11 @@ __device__ __forceinline__ double d4(const double *p, long long c, long long s)
   return dfc<ODR>(p[c - s], p[c], p[c + s], p[c + 2 * s]);
 }
 
+// update cell (i,j,k), i in [GH, nx-GH] etc.: the extra face of the staggered fields included
 template <int ODR>
-__global__ void k_update(View v, double c0, double c1)
+__device__ __forceinline__ void update_body(const View &v, int i, int j, int k, double c0, double c1)
 {
-  if (v.ctl->done) return;
   const Geo &g = v.g;
-  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z * blockDim.z + threadIdx.z;
-  if (i > g.nx - GH) return;
-  if (g.dim >= 2 && j > g.ny - GH) return;
-  if (g.dim >= 3 && k > g.nz - GH) return;
-  if (g.dim < 2 && j > 0) return;
-  if (g.dim < 3 && k > 0) return;
   const long long c = cidx(g, i, j, k);
   const double dtdx = v.ctl->dtd[0], dtdy = v.ctl->dtd[1], dtdz = v.ctl->dtd[2];
   const bool ci = i < g.nx - GH;
@@ -633,6 +650,31 @@ __global__ void k_update(View v, double c0, double c1)
   }
 }
 
+// offset of the update launch: threads start at the first interior cell
+__device__ __forceinline__ bool update_cell(const Geo &g, int ti, int tj, int tk, int &i, int &j, int &k)
+{
+  i = GH + ti;
+  j = (g.dim >= 2 ? GH : 0) + tj;
+  k = (g.dim >= 3 ? GH : 0) + tk;
+  if (i > g.nx - GH) return false;
+  if (g.dim >= 2 && j > g.ny - GH) return false;
+  if (g.dim >= 3 && k > g.nz - GH) return false;
+  if (g.dim < 2 && j > 0) return false;
+  if (g.dim < 3 && k > 0) return false;
+  return true;
+}
+
+template <int ODR>
+__global__ void k_update(View v, double c0, double c1)
+{
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!update_cell(v.g, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
+                   blockIdx.z * blockDim.z + threadIdx.z, i, j, k))
+    return;
+  update_body<ODR>(v, i, j, k, c0, c1);
+}
+
 // ---------------------------------------------------------------------------
 // ghost fill of the state (bound()), launched over the ghost shell only: the
 // cells with an index in [0,GH) or [n-GH,n) along some active axis
@@ -681,13 +723,8 @@ __device__ __forceinline__ void shell_cell(const Geo &g, long long t, int &i, in
   i = col < GH ? col : g.nx - 2 * GH + col;
 }
 
-__global__ void k_bound(View v)
+__device__ __forceinline__ void bound_body(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= shell_cells(v.g)) return;
-  int i, j, k;
-  shell_cell(v.g, t, i, j, k);
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
 #pragma unroll
@@ -702,11 +739,21 @@ __global__ void k_bound(View v)
   }
 }
 
+__global__ void k_bound(View v)
+{
+  if (v.ctl->done) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= shell_cells(v.g)) return;
+  int i, j, k;
+  shell_cell(v.g, t, i, j, k);
+  bound_body(v, i, j, k);
+}
+
 // ---------------------------------------------------------------------------
 // exec_ loop control and setdt
 // ---------------------------------------------------------------------------
 // begin of a loop iteration: the while() test of exec_, tim += dt, dt/dx
-__global__ void k_begin_step(View v, int check_tim)
+__device__ __forceinline__ void begin_body(const View &v, int check_tim)
 {
   Ctl *c = v.ctl;
   if (c->done) return;
@@ -721,6 +768,7 @@ __global__ void k_begin_step(View v, int check_tim)
   c->dtd[1] = v.g.dim >= 2 ? c->dt / v.dy : 0.0;
   c->dtd[2] = v.g.dim >= 3 ? c->dt / v.dz : 0.0;
 }
+__global__ void k_begin_step(View v, int check_tim) { begin_body(v, check_tim); }
 
 // dt/dx etc. for a host-supplied dt (qas_step)
 __global__ void k_set_dt(View v, double dt)
@@ -738,18 +786,11 @@ __global__ void k_vmax_reset(View v)
   v.ctl->vmax_bits = (unsigned long long)__double_as_longlong(1.0);
 }
 
-// max over the interior of |v| + c_f with B from the 2nd-order face average
-// (mhd2d_class.cpp:17-26); NaN never wins, as with `if (vtmp > vmax)`.
-__global__ void k_vmax(View v)
+// |v| + c_f at interior cell (i,j,k) with B from the 2nd-order face average (setdt)
+__device__ __forceinline__ double vmax_cell(const View &v, int i, int j, int k)
 {
-  if (v.ctl->done) return;
   const Geo &g = v.g;
-  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
-  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
-  double best = 1.0;
-  if (i < g.nx - GH) {
-    const long long c = cidx(g, i, j, k);
+  const long long c = cidx(g, i, j, k);
     double cx, cy, cz;
     if (g.dim == 1) {
       cx = v.u[4][c];
@@ -774,6 +815,21 @@ __global__ void k_vmax(View v)
       vt = sqrt(vx * vx + vy * vy) + vf;
     else
       vt = sqrt(vx * vx + vy * vy + vz * vz) + vf;
+    return vt;
+}
+
+// max over the interior of |v| + c_f with B from the 2nd-order face average
+// (mhd2d_class.cpp:17-26); NaN never wins, as with `if (vtmp > vmax)`.
+__global__ void k_vmax(View v)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (g.dim >= 2 ? GH : 0) + blockIdx.y;
+  const int k = (g.dim >= 3 ? GH : 0) + blockIdx.z;
+  double best = 1.0;
+  if (i < g.nx - GH) {
+    const double vt = vmax_cell(v, i, j, k);
     if (vt > best) best = vt;
   }
 #pragma unroll
@@ -798,7 +854,7 @@ __global__ void k_vmax(View v)
 
 // dt = cfl*dr/vmax; on the first call also exec_'s nmax (mhd2d_class.cpp:27-32,
 // mhd1d_class.cpp:146-151)
-__global__ void k_setdt(View v, double cfl, double dr, int rule, double dtrec, int nout)
+__device__ __forceinline__ void setdt_body(const View &v, double cfl, double dr, int rule, double dtrec, int nout)
 {
   Ctl *c = v.ctl;
   if (c->done) return;
@@ -813,6 +869,10 @@ __global__ void k_setdt(View v, double cfl, double dr, int rule, double dtrec, i
     }
     c->first = 0;
   }
+}
+__global__ void k_setdt(View v, double cfl, double dr, int rule, double dtrec, int nout)
+{
+  setdt_body(v, cfl, dr, rule, dtrec, nout);
 }
 
 // |div B| with df1[ODR-1] over the interior; max by bit pattern of non-negative doubles

@@ -32,7 +32,9 @@ EXPORTS = (
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
     "qas_run", "qas_run_reset", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
-    "qas_get_tile", "qas_autotune",
+    "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
+    "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
+    "qas_batch_stream", "qas_batch_kernel_launches",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -123,6 +125,17 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_set_tile.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.qas_get_tile.argtypes = [vp, ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 3
     lib.qas_autotune.argtypes = [vp, ctypes.c_int]
+    lib.qas_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(Grid), ctypes.POINTER(Scheme),
+                                     ctypes.POINTER(BC), ctypes.c_int]
+    lib.qas_batch_destroy.argtypes = [vp]
+    lib.qas_batch_cells.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    lib.qas_batch_upload.argtypes = [vp, ctypes.c_int, dp]
+    lib.qas_batch_download.argtypes = [vp, ctypes.c_int, dp]
+    lib.qas_batch_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
+    lib.qas_batch_set_tile.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qas_batch_autotune.argtypes = [vp, ctypes.c_int]
+    lib.qas_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.qas_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -308,3 +321,84 @@ def bc_map(prob, group: int, field: int, axis: int):
     _check(lib.qas_bc_map(ctypes.byref(g), ctypes.byref(b), group, field, axis,
                           src.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(fac), n), "qas_bc_map")
     return src, fac
+
+
+def _grid_scheme_bc(prob):
+    g = Grid(prob.dim, prob.nxm, prob.nym if prob.dim >= 2 else 1, prob.nzm if prob.dim >= 3 else 1, prob.dx,
+             prob.dy if prob.dim >= 2 else 0.0, prob.dz if prob.dim >= 3 else 0.0, prob.gam)
+    sc = Scheme(prob.rmn, prob.odr, prob.rk, prob.ctw)
+    b = BC()
+    for m in range(8):
+        b.dnx[m], b.dny[m], b.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+    return g, sc, b
+
+
+class Batch:
+    """An ensemble of independent problems stepped together (qas_batch_*)."""
+
+    def __init__(self, probs, device: int = -1):
+        self.lib = load()
+        n = len(probs)
+        gs, ss, bs = (Grid * n)(), (Scheme * n)(), (BC * n)()
+        for q, p in enumerate(probs):
+            gs[q], ss[q], bs[q] = _grid_scheme_bc(p)
+        h = ctypes.c_void_p()
+        _check(self.lib.qas_batch_create(ctypes.byref(h), n, gs, ss, bs, device), "qas_batch_create")
+        self.h = h
+        self.n = n
+        self.nd = []
+        for q in range(n):
+            v = ctypes.c_longlong()
+            _check(self.lib.qas_batch_cells(self.h, q, ctypes.byref(v)), "qas_batch_cells")
+            self.nd.append(int(v.value))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.qas_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, q: int, state: np.ndarray) -> None:
+        st = np.ascontiguousarray(state, dtype=np.float64).reshape(-1)
+        assert st.size == 8 * self.nd[q]
+        _check(self.lib.qas_batch_upload(self.h, q, _dptr(st)), "qas_batch_upload")
+
+    def download(self, q: int, shape=None) -> np.ndarray:
+        out = np.empty(8 * self.nd[q], dtype=np.float64)
+        _check(self.lib.qas_batch_download(self.h, q, _dptr(out)), "qas_batch_download")
+        return out if shape is None else out.reshape(shape)
+
+    def run(self, max_steps: int = 0, flg: int = 1, stop_rule: int = 0, cfl: float = 0.4, dtrec: float = 1.0,
+            nout: int = 1, use_graph: bool = True):
+        o = RunOpts(int(max_steps), int(flg), int(stop_rule), float(cfl), float(dtrec), int(nout),
+                    1 if use_graph else 0, 0.0, 0.0)
+        info = (RunInfo * self.n)()
+        _check(self.lib.qas_batch_run(self.h, ctypes.byref(o), info), "qas_batch_run")
+        return [(info[q].steps, info[q].tim, info[q].dt) for q in range(self.n)]
+
+    def set_tile(self, kernel: str, tx: int, ty: int = 1, tz: int = 1) -> None:
+        _check(self.lib.qas_batch_set_tile(self.h, kernel.encode(), tx, ty, tz), "qas_batch_set_tile")
+
+    def autotune(self, trial_steps: int = 2) -> None:
+        _check(self.lib.qas_batch_autotune(self.h, int(trial_steps)), "qas_batch_autotune")
+
+    def stream(self) -> int:
+        v = ctypes.c_void_p()
+        _check(self.lib.qas_batch_stream(self.h, ctypes.byref(v)), "qas_batch_stream")
+        return int(v.value or 0)
+
+    def kernel_launches(self) -> int:
+        v = ctypes.c_longlong()
+        _check(self.lib.qas_batch_kernel_launches(self.h, ctypes.byref(v)), "qas_batch_kernel_launches")
+        return int(v.value)

@@ -292,3 +292,29 @@ def smooth_wave(dim: int, n: int, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3
     st = _pack(ro, vx, vy, vz, bx, by, bz, pr, bx, by, bz, p.gam)
     p.state = st
     return p
+
+
+# ----------------------------------------------------------------------------
+# C4: batched ensemble
+# ----------------------------------------------------------------------------
+
+def ensemble(n: int = 512, lo: int = 64, hi: int = 512, seed: int = 2025, odr: int = 4) -> list:
+    """Seeded ensemble of 2D instances with log-uniform sides in [lo, hi]
+    (non-square allowed): even members are Orszag-Tang (HLLD), odd members
+    Kelvin-Helmholtz (MLAU) with Mach number log-uniform in [1e-3, 1] and
+    plasma beta log-uniform in [0.1, 1e3]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        nx = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        ny = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        if q % 2 == 0:
+            p = orszag_tang(nx, nym=ny, rmn=RMN_HLLD, odr=odr)
+        else:
+            mach = math.exp(rng.uniform(math.log(1e-3), math.log(1.0)))
+            beta = math.exp(rng.uniform(math.log(0.1), math.log(1e3)))
+            p = kelvin_helmholtz(2, nx, nym=ny, mach=mach, beta=beta, rmn=RMN_MLAU, odr=odr,
+                                 seed=int(rng.integers(1 << 30)))
+        p.name = f"ens{q}_{p.name}"
+        out.append(p)
+    return out
