@@ -28,6 +28,20 @@ import numpy as np  # noqa: E402
 
 ALG_BYTES_PER_CELL_UPDATE = 512  # 8 FP64 fields: stage 1 reads u^n, writes; stages 2-3 read stage input + u^n, write
 
+# Dominant kernel k_lr (characteristic WCNS face states of one direction): algorithmic
+# FP64 arrays per cell: reads ro,vn,vt,vu,bt,bu,pr, the centre normal field and the face
+# normal field (9); writes the 7+7 face states and the CUCT induction states (2 in 2D,
+# 4 in 3D).
+K_LR_ARRAYS = {1: 8 + 14, 2: 9 + 16, 3: 9 + 18}
+# FP64 work of k_lr per cell, counted by ncu on the 2D Orszag-Tang 1024^2 workload
+# (ODR=4; profiles/k_lr_ot2d_1024.md): dadd + dmul + dfma instructions and flops
+# (a dfma counts 2).
+K_LR_FP64_INSTR_PER_CELL = 1054.0
+K_LR_FP64_FLOPS_PER_CELL = 1262.0
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_lr launch (y direction) on the
+# same workload (profiles/k_lr_ot2d_1024.md)
+K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.76e6 + 99.48e6}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -38,6 +52,8 @@ def parse():
     ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "bw1d_1024"], default="ot2d_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -122,6 +138,53 @@ def cpu_baseline(prob, steps=3, threads=None):
             "kind": "reference",
             "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, "
                       f"reference -O2 -fopenmp, OMP_NUM_THREADS={threads}"}
+
+
+def ensemble_compare(steps):
+    """Batched ensemble (512 seeded 2D instances, log-uniform sides 64..512, half
+    Orszag-Tang/HLLD, half Kelvin-Helmholtz/MLAU) in one launch sequence per step,
+    against the same instances run one after another through the plain path (each
+    with its own graph-captured exec_ loop).  Device time by CUDA events."""
+    import torch
+
+    from qasmhd_b200 import lib as L
+    from qasmhd_b200 import problems as P
+    probs = P.ensemble(512)
+    cells = sum(p.interior_cells for p in probs)
+    b = L.Batch(probs)
+    for q, p in enumerate(probs):
+        b.upload(q, p.state)
+    b.autotune(1)
+    b.run(max_steps=2, flg=1, stop_rule=0, cfl=0.4)
+    ext = torch.cuda.ExternalStream(b.stream())
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.kernel_launches()
+    s0.record(ext)
+    b.run(max_steps=steps, flg=1, stop_rule=0, cfl=0.4)
+    s1.record(ext)
+    s1.synchronize()
+    ms_b = s0.elapsed_time(s1)
+    launches_b = b.kernel_launches() - l0
+    b.close()
+    ms_p = 0.0
+    launches_p = 0
+    for p in probs:
+        with L.Context.from_problem(p) as c:
+            c.upload(p.state)
+            c.run(max_steps=2, flg=1, stop_rule=0, cfl=0.4)
+            ext = torch.cuda.ExternalStream(c.stream())
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = c.kernel_launches()
+            s0.record(ext)
+            c.run(max_steps=steps, flg=1, stop_rule=0, cfl=0.4)
+            s1.record(ext)
+            s1.synchronize()
+            ms_p += s0.elapsed_time(s1)
+            launches_p += c.kernel_launches() - l0
+    return {"workload": "ensemble_512_2d_64-512_OT-HLLD_KH-MLAU", "instances": len(probs), "cells": cells,
+            "steps": steps, "batched_mcells": cells * steps / ms_b / 1e3,
+            "per_instance_mcells": cells * steps / ms_p / 1e3, "ratio": ms_p / ms_b,
+            "batched_launches": launches_b, "per_instance_launches": launches_p}
 
 
 def run_reference_arm(args):
@@ -232,7 +295,22 @@ def main():
     except Exception:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = ALG_BYTES_PER_CELL_UPDATE * cells / (ms_step * 1e-3) / 1e9
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    step_gbs = ALG_BYTES_PER_CELL_UPDATE * cells / (ms_step * 1e-3) / 1e9
+
+    # dominant kernel, timed live with CUDA events on the context's stream over
+    # min(K, 10) eager steps after the timed region
+    prof = ctx.profile(min(args.steps, 10), flg=1, cfl=prob.cfl)
+    dom = max(prof, key=lambda k: prof[k][1])
+    dom_launches, dom_ms = prof[dom]
+    dom_ms_launch = dom_ms / dom_launches
+    step_prof_ms = sum(v[1] for v in prof.values())
+    lr_cells = prob.nd  # k_lr covers every cell but two ghost layers per side along its axis
+    lr_bytes = K_LR_ARRAYS[prob.dim] * 8.0 * lr_cells
+    achieved = lr_bytes / (dom_ms_launch * 1e-3) / 1e9 if dom == "k_lr" else None
+    fp64_peak = L.fp64_peak_tflops()
+    lr_tflops = K_LR_FP64_FLOPS_PER_CELL * lr_cells / (dom_ms_launch * 1e-3) / 1e12
+    lr_pipe = K_LR_FP64_INSTR_PER_CELL * lr_cells / (dom_ms_launch * 1e-3) / (fp64_peak * 1e12 / 2.0)
     line = {
         "metric": "Mcell-updates/s/GPU FP64 (per-step update)", "value": value, "unit": "Mcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -240,15 +318,29 @@ def main():
         "data": "synthetic (seeded initial state of the named problem)",
         "config": dict(cfg, parallelism=f"replicas{world}",
                        l2="working set per step ~%.2f GB > 126 MB L2" % (77 * prob.nd * 8 / 1e9)),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
-                     "basis": "whole step, 512 algorithmic B per cell-update, peak of measured"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": (achieved / hbm_peak) if achieved else None,
+                     "traffic": K_LR_TRAFFIC_PER_LAUNCH.get(args.workload),
+                     "launch_ms": dom_ms_launch, "share_of_step": dom_ms / step_prof_ms,
+                     "basis": f"algorithmic {K_LR_ARRAYS[prob.dim]} FP64 arrays per cell per launch / live "
+                              f"CUDA-event launch time; peak of {peak_src}; traffic = ncu dram read+write "
+                              "per launch"},
+        "fp64": {"kernel": "k_lr", "achieved_tflops": lr_tflops, "peak_tflops": fp64_peak,
+                 "frac": lr_tflops / fp64_peak, "pipe_frac": lr_pipe,
+                 "basis": "ncu-counted FP64 flops per cell x cells / live launch time; peak = measured DFMA "
+                          "throughput (qas_fp64_peak); pipe_frac = FP64 instructions vs the DFMA issue rate"},
+        "step_roofline": {"achieved": step_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": step_gbs / hbm_peak,
+                          "basis": "whole step, 512 algorithmic B per cell-update"},
+        "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
         "e2e": {"value": e_value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb},
         "gpu_launches": launches,
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(prob)
+    if rank == 0 and not args.no_ensemble and world == 1:
+        ctx.close()
+        line["batched"] = ensemble_compare(args.ensemble_steps)
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -195,6 +195,11 @@ qas_status qas_get_tile(const qas_ctx *ctx, const char *kernel, int *tx, int *ty
  * Choices are cached per (dim, ODR, RMN, grid-size bucket) for the life of the process. */
 qas_status qas_autotune(qas_ctx *ctx, int trial_steps);
 
+/* Diagnostics: measured FP64 throughput of the current device (TFLOP/s, FMA = 2 flops),
+ * from independent DFMA chains on every SM timed with CUDA events; the FP64 roof of the
+ * step's kernels. */
+qas_status qas_fp64_peak(double *tflops);
+
 /* Number of kernels this context has launched (eager launches plus kernels inside
  * replayed graphs), for launch accounting. */
 qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);

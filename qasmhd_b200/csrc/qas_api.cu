@@ -1125,6 +1125,33 @@ qas_status qas_autotune(qas_ctx *c, int trial_steps)
   return QAS_OK;
 }
 
+qas_status qas_fp64_peak(double *tflops)
+{
+  if (!tflops) return QAS_ERR_INVALID;
+  int dev = 0, sms = 0;
+  QAS_CUDA(cudaGetDevice(&dev));
+  QAS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  double *d = nullptr;
+  QAS_CUDA(cudaMalloc(&d, sizeof(double)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = sms * 8, iters = 20000;
+  k_fp64_peak<<<blocks, threads>>>(d, 1000, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(e0);
+  k_fp64_peak<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "fp64 peak");
+  *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (ms * 1e-3) / 1e12;
+  return QAS_OK;
+}
+
 qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 {
   if (!c || !count) return QAS_ERR_INVALID;

@@ -899,4 +899,17 @@ __global__ void k_divb(View v, unsigned long long *out)
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(d));
 }
 
+// FP64 throughput probe: 8 independent DFMA chains per thread (2 flops each)
+__global__ void k_fp64_peak(double *out, int iters, double a, double b)
+{
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1.0, x2 = x0 + 2.0, x3 = x0 + 3.0;
+  double x4 = x0 + 4.0, x5 = x0 + 5.0, x6 = x0 + 6.0, x7 = x0 + 7.0;
+  for (int it = 0; it < iters; it++) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  const double r = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (r == 12345.0) out[0] = r;  // keeps the chains live
+}
+
 }  // namespace qas

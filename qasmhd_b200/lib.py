@@ -34,7 +34,7 @@ EXPORTS = (
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
-    "qas_batch_stream", "qas_batch_kernel_launches",
+    "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -136,6 +136,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_batch_autotune.argtypes = [vp, ctypes.c_int]
     lib.qas_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.qas_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.qas_fp64_peak.argtypes = [dp]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -402,3 +403,11 @@ class Batch:
         v = ctypes.c_longlong()
         _check(self.lib.qas_batch_kernel_launches(self.h, ctypes.byref(v)), "qas_batch_kernel_launches")
         return int(v.value)
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 throughput of the current device (qas_fp64_peak)."""
+    lib = load()
+    v = ctypes.c_double()
+    _check(lib.qas_fp64_peak(ctypes.byref(v)), "qas_fp64_peak")
+    return v.value
