@@ -228,6 +228,27 @@ qas_status qas_batch_autotune(qas_batch *batch, int trial_steps);
 qas_status qas_batch_stream(qas_batch *batch, void **stream);
 qas_status qas_batch_kernel_launches(const qas_batch *batch, long long *count);
 
+/* ------------------------------------------------------------------------------------
+ * Discrete adjoint of the 2D step (no counterpart in the reference, which has no
+ * derivatives): the exec_ step body -- bound(), ideal(dt) (MHD2D::ideal,
+ * 2D/SERIAL/OTvortex/mhd2d_solve.cpp:3-400) and, with eta0 > 0, setdc + the sub-cycled
+ * DMHD2D::dsptv (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26) with uniform eta and nu = 0 --
+ * for RMN = Roe, ODR = 4 (characteristic WCNS4), any R_K, CTW and valid boundary flags.
+ *
+ * qas_adjoint_forward runs `nsteps` steps from the current device state with the given
+ * dt per step (dts[nsteps], host), keeping a snapshot every `ckpt_every` steps; the state
+ * afterwards is the final state (bit-identical to qas_run with the same dt sequence).
+ * qas_adjoint_backward takes dL/d(final state) (host, 8*nd doubles, field-major like
+ * qas_download_block) and returns dL/d(initial state) in the same layout and dL/deta0
+ * (may be NULL).  It recomputes each checkpoint segment with its intermediates recorded
+ * on a device tape and reverses it; dt and the sub-cycle counts are held fixed.  The
+ * context's state is the forward run's final state again when it returns.
+ * Status: QAS_ERR_UNSUPPORTED for other dims/solvers/orders or more than 8 sub-cycles,
+ * QAS_ERR_INVALID for a backward call without a forward run.
+ * ------------------------------------------------------------------------------------ */
+qas_status qas_adjoint_forward(qas_ctx *ctx, int nsteps, int ckpt_every, const double *dts, double eta0);
+qas_status qas_adjoint_backward(qas_ctx *ctx, const double *dldu_final, double *dldu0, double *dldeta0);
+
 #ifdef __cplusplus
 }
 #endif

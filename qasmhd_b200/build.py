@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqas.so")
 SOURCES = ["qas_api.cu"]
-HEADERS = ["qas_device.cuh", "qas_kernels.cuh", "qas_dissip.cuh", "qas_batch.cuh", "qas_batch_api.inc"]
+HEADERS = ["qas_device.cuh", "qas_kernels.cuh", "qas_dissip.cuh", "qas_batch.cuh", "qas_batch_api.inc",
+           "qas_adjoint.cuh", "qas_adjoint_kernels.cuh", "qas_adjoint_api.inc"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

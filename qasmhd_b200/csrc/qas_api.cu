@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/qas.h"
+#include "qas_adjoint_kernels.cuh"
 #include "qas_batch.cuh"
 #include "qas_dissip.cuh"
 #include "qas_kernels.cuh"
@@ -41,6 +42,9 @@ qas_status cuda_fail(cudaError_t e, const char *what)
 double hmin(double a, double b) { return (a >= b) ? b : a; }  // common/common_func.h:11-15
 
 }  // namespace
+
+struct AdjState;  // discrete-adjoint run state (qas_adjoint_api.inc)
+static void adj_free(qas_ctx *c);
 
 struct qas_ctx {
   int device = 0;
@@ -82,6 +86,7 @@ struct qas_ctx {
   std::vector<int> prof_kids;  // kernel id of each recorded pair
   double prof_ms[32] = {0};
   long long prof_n[32] = {0};
+  AdjState *adj = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -586,6 +591,7 @@ qas_status qas_destroy(qas_ctx *c)
 {
   if (!c) return QAS_ERR_INVALID;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  adj_free(c);
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
   if (c->pool) cudaFree(c->pool);
@@ -1162,3 +1168,4 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 }  // extern "C"
 
 #include "qas_batch_api.inc"
+#include "qas_adjoint_api.inc"

@@ -10,17 +10,22 @@
 // template parameter and the stencils live in registers.
 #pragma once
 
-#include <cuda_runtime.h>
 #include <math.h>
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#define QAS_HD __host__ __device__ __forceinline__
+#else
+#define QAS_HD inline
+#endif
 
 namespace qas {
 
 // ---------------------------------------------------------------------------
 // common/common_func.h:4-31
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double qmax(double a, double b) { return (a >= b) ? a : b; }
-__device__ __forceinline__ double qmin(double a, double b) { return (a >= b) ? b : a; }
-__device__ __forceinline__ double minmod(double a, double b)
+QAS_HD double qmax(double a, double b) { return (a >= b) ? a : b; }
+QAS_HD double qmin(double a, double b) { return (a >= b) ? b : a; }
+QAS_HD double minmod(double a, double b)
 {
   return +qmin(qmax(a, b), 0.0) + qmax(qmin(a, b), 0.0);
 }
@@ -30,13 +35,13 @@ __device__ __forceinline__ double minmod(double a, double b)
 // f0 is the value at face i-1/2, f1 at i+1/2, fm at i-3/2, f2 at i+3/2.
 // ---------------------------------------------------------------------------
 template <int ODR>
-__device__ __forceinline__ double fcen(double fm, double f0, double f1, double f2)
+QAS_HD double fcen(double fm, double f0, double f1, double f2)
 {
   if (ODR >= 3) return (0.0625 * (9.0 * (f0 + f1) - (fm + f2)));
   return (0.5 * (f0 + f1));
 }
 template <int ODR>
-__device__ __forceinline__ double dfc(double fm, double f0, double f1, double f2)
+QAS_HD double dfc(double fm, double f0, double f1, double f2)
 {
   if (ODR >= 3) return ((27.0 * (f1 - f0) - (f2 - fm)) / 24.0);
   return (f1 - f0);
@@ -47,7 +52,7 @@ __device__ __forceinline__ double dfc(double fm, double f0, double f1, double f2
 // f[0..4] = values at i-2..i+2; fl at i+1/2, fr at i-1/2
 // ---------------------------------------------------------------------------
 template <int ODR>
-__device__ __forceinline__ void lin_lr(const double f[5], double &fl, double &fr)
+QAS_HD void lin_lr(const double f[5], double &fl, double &fr)
 {
   if (ODR == 1) {
     fl = f[2];
@@ -64,14 +69,14 @@ __device__ __forceinline__ void lin_lr(const double f[5], double &fl, double &fr
   }
 }
 template <int ODR>
-__device__ __forceinline__ double lin_left(const double f[5])
+QAS_HD double lin_left(const double f[5])
 {
   double l, r;
   lin_lr<ODR>(f, l, r);
   return l;
 }
 template <int ODR>
-__device__ __forceinline__ double lin_right(const double f[5])
+QAS_HD double lin_right(const double f[5])
 {
   double l, r;
   lin_lr<ODR>(f, l, r);
@@ -83,7 +88,7 @@ __device__ __forceinline__ double lin_right(const double f[5])
 // 1st order, MUSCL minmod (common_interp.c:32-37), WCNS3 (:65-101),
 // WCNS4 (:102-150)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void wcns4_lr(const double f[5], double &fl, double &fr)
+QAS_HD void wcns4_lr(const double f[5], double &fl, double &fr)
 {
   const double eps = 1e-40;
   double c1, c2;
@@ -122,7 +127,7 @@ __device__ __forceinline__ void wcns4_lr(const double f[5], double &fl, double &
   fr = 0.125 * (+w2 * pr2 + w1 * pr1 + w0 * pr0);
 }
 
-__device__ __forceinline__ void wcns3_lr(const double f[5], double &fl, double &fr)
+QAS_HD void wcns3_lr(const double f[5], double &fl, double &fr)
 {
   const double eps = 1e-40;
   double c1 = f[1] - f[2];
@@ -145,7 +150,7 @@ __device__ __forceinline__ void wcns3_lr(const double f[5], double &fl, double &
 }
 
 template <int ODR>
-__device__ __forceinline__ void nl_lr(const double f[5], double &fl, double &fr)
+QAS_HD void nl_lr(const double f[5], double &fl, double &fr)
 {
   if (ODR == 1) {
     fl = f[2];
@@ -170,7 +175,7 @@ __device__ __forceinline__ void nl_lr(const double f[5], double &fl, double &fr)
 // (:175-434), projections written sparsely.
 // ---------------------------------------------------------------------------
 template <int ODR>
-__device__ __forceinline__ void face_states(const double q[7][5], double bn, double gam, double vl[7],
+QAS_HD void face_states(const double q[7][5], double bn, double gam, double vl[7],
                                             double vr[7])
 {
   const double ro = q[0][2], vn = q[1][2], vt = q[2][2], vu = q[3][2];
@@ -273,7 +278,7 @@ __device__ __forceinline__ void face_states(const double q[7][5], double bn, dou
 // `P` is a functor P(v, m) returning primitive v at stencil point m.
 // ---------------------------------------------------------------------------
 template <int ODR, class Stencil>
-__device__ __forceinline__ void face_states_grouped(const Stencil &P, double bn, double gam, double vl[7],
+QAS_HD void face_states_grouped(const Stencil &P, double bn, double gam, double vl[7],
                                                     double vr[7])
 {
   const double ro = P(0, 2), vn = P(1, 2), vt = P(2, 2), vu = P(3, 2);
@@ -388,7 +393,7 @@ __device__ __forceinline__ void face_states_grouped(const Stencil &P, double bn,
 
 // HLLD (LOW=false, mhd_flux.c:435-561) and low-dissipation LHLLD (LOW=true, :563-698)
 template <bool LOW>
-__device__ __forceinline__ void flux_hlld(const double L[7], const double R[7], double bnc, double gamma,
+QAS_HD void flux_hlld(const double L[7], const double R[7], double bnc, double gamma,
                                           double dv0, double dv1, double F[7])
 {
   const double rol = L[0], vnl = L[1], vtl = L[2], vul = L[3], btl = L[4], bul = L[5], prl = L[6];
@@ -510,7 +515,7 @@ __device__ __forceinline__ void flux_hlld(const double L[7], const double R[7], 
 }
 
 // MLAU all-speed flux, common/mhd_flux.c:7-192
-__device__ __forceinline__ void flux_mlau(const double L[7], const double R[7], double bnc, double gamma,
+QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double gamma,
                                           double dv0, double dv1, double F[7])
 {
   const double rol = L[0], vnl = L[1], vtl = L[2], vul = L[3], btl = L[4], bul = L[5], prl = L[6];
@@ -671,7 +676,7 @@ __device__ __forceinline__ void flux_mlau(const double L[7], const double R[7], 
 }
 
 // Roe flux, common/mhd_flux.c:194-433
-__device__ __forceinline__ void flux_roe(const double L[7], const double R[7], double bnc, double gamma, double F[7])
+QAS_HD void flux_roe(const double L[7], const double R[7], double bnc, double gamma, double F[7])
 {
   const double rol = L[0], vnl = L[1], vtl = L[2], vul = L[3], btl = L[4], bul = L[5], prl = L[6];
   const double ror = R[0], vnr = R[1], vtr = R[2], vur = R[3], btr = R[4], bur = R[5], prr = R[6];
@@ -834,7 +839,7 @@ __device__ __forceinline__ void flux_roe(const double L[7], const double R[7], d
 }
 
 template <int RMN>
-__device__ __forceinline__ void riemann(const double L[7], const double R[7], double bnc, double gamma, double dv0,
+QAS_HD void riemann(const double L[7], const double R[7], double bnc, double gamma, double dv0,
                                         double dv1, double F[7])
 {
   if (RMN == 0)
@@ -850,7 +855,7 @@ __device__ __forceinline__ void riemann(const double L[7], const double R[7], do
 // CUCT corner weight, common/mhd_func.c:56-76. Arguments are the values at the
 // four cells (a-1,b-1),(a,b-1),(a-1,b),(a,b) of the corner's plane, ba at
 // (a,b-1),(a,b) and bb at (a-1,b),(a,b).
-__device__ __forceinline__ double cuct_weight(double r0, double r1, double r2, double r3, double va0, double va1,
+QAS_HD double cuct_weight(double r0, double r1, double r2, double r3, double va0, double va1,
                                               double va2, double va3, double vb0, double vb1, double vb2, double vb3,
                                               double ba1, double ba3, double bb2, double bb3)
 {
@@ -867,7 +872,7 @@ __device__ __forceinline__ double cuct_weight(double r0, double r1, double r2, d
 }
 
 // SSP-RK combine, common/common_func.h:28-31
-__device__ __forceinline__ double rk_combine(double f1, double f0, double df, double c0, double c1)
+QAS_HD double rk_combine(double f1, double f0, double df, double c0, double c1)
 {
   return c0 * f0 + c1 * (f1 + df);
 }

@@ -34,7 +34,8 @@ EXPORTS = (
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
-    "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak",
+    "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
+    "qas_adjoint_backward",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -137,6 +138,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.qas_batch_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.qas_fp64_peak.argtypes = [dp]
+    lib.qas_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double]
+    lib.qas_adjoint_backward.argtypes = [vp, dp, dp, dp]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -289,6 +292,23 @@ class Context:
     def dsptv(self, dt: float, nu0: float, eta0: float) -> None:
         _check(self.lib.qas_dsptv(self.h, float(dt), float(nu0), float(eta0)), "qas_dsptv")
 
+    # discrete adjoint ---------------------------------------------------------
+    def adjoint_forward(self, dts: Sequence[float], eta0: float = 0.0, ckpt_every: int = 20) -> None:
+        """Run len(dts) exec_ steps (bound, ideal, dissipate) from the device state with the
+        given dt per step, keeping checkpoints for adjoint_backward."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        _check(self.lib.qas_adjoint_forward(self.h, int(d.size), int(ckpt_every), _dptr(d), float(eta0)),
+               "qas_adjoint_forward")
+
+    def adjoint_backward(self, dldu: np.ndarray):
+        """dL/d(final state) (8*nd values) -> (dL/d(initial state) as (8, nd), dL/deta0)."""
+        g = np.ascontiguousarray(dldu, dtype=np.float64).reshape(8, -1)
+        assert g.shape[1] == self.nd
+        out = np.empty((8, self.nd), dtype=np.float64)
+        eb = ctypes.c_double()
+        _check(self.lib.qas_adjoint_backward(self.h, _dptr(g), _dptr(out), ctypes.byref(eb)), "qas_adjoint_backward")
+        return out, eb.value
+
     def max_divb(self) -> float:
         v = ctypes.c_double()
         _check(self.lib.qas_max_divb(self.h, ctypes.byref(v)), "qas_max_divb")
@@ -411,3 +431,4 @@ def fp64_peak_tflops() -> float:
     v = ctypes.c_double()
     _check(lib.qas_fp64_peak(ctypes.byref(v)), "qas_fp64_peak")
     return v.value
+
