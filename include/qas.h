@@ -249,6 +249,22 @@ qas_status qas_batch_kernel_launches(const qas_batch *batch, long long *count);
 qas_status qas_adjoint_forward(qas_ctx *ctx, int nsteps, int ckpt_every, const double *dts, double eta0);
 qas_status qas_adjoint_backward(qas_ctx *ctx, const double *dldu_final, double *dldu0, double *dldeta0);
 
+/* ------------------------------------------------------------------------------------
+ * Allocation-free max |div B| (no counterpart in the reference, whose caller owns host
+ * arrays and never allocates device memory): the same value as qas_max_divb, for a state
+ * the caller already holds in device memory, without a context and without allocating.
+ * d_state: 8 fields of the reference's ghost-padded layout, field m at d_state +
+ * m*field_stride (field_stride >= nd); stream: a cudaStream_t (NULL = default stream);
+ * synchronises that stream.  Scratch is a static device array sized for
+ * QAS_NOALLOC_MAX_ROWS interior rows (nym*nzm); larger grids return QAS_ERR_UNSUPPORTED
+ * with the reason in qas_last_cuda_error().  The first call on a device resolves the
+ * scratch address (module loading may allocate): make it before any stream capture.
+ * Calls that overlap in time on one device share the scratch and race: serialise them.
+ * ------------------------------------------------------------------------------------ */
+#define QAS_NOALLOC_MAX_ROWS 65536
+qas_status qas_max_divb_noalloc(const qas_grid *grid, int odr, const double *d_state, long long field_stride,
+                                void *stream, double *maxdivb);
+
 #ifdef __cplusplus
 }
 #endif

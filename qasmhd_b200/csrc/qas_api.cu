@@ -1169,3 +1169,4 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 
 #include "qas_batch_api.inc"
 #include "qas_adjoint_api.inc"
+#include "qas_noalloc.inc"

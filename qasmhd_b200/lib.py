@@ -35,7 +35,7 @@ EXPORTS = (
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
     "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
-    "qas_adjoint_backward",
+    "qas_adjoint_backward", "qas_max_divb_noalloc",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -140,6 +140,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_fp64_peak.argtypes = [dp]
     lib.qas_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double]
     lib.qas_adjoint_backward.argtypes = [vp, dp, dp, dp]
+    lib.qas_max_divb_noalloc.argtypes = [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                         ctypes.c_void_p, dp]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
     for name in EXPORTS:
@@ -432,3 +434,13 @@ def fp64_peak_tflops() -> float:
     _check(lib.qas_fp64_peak(ctypes.byref(v)), "qas_fp64_peak")
     return v.value
 
+
+def max_divb_noalloc(grid: "Grid", odr: int, d_state_ptr: int, field_stride: int, stream: int = 0) -> float:
+    """qas_max_divb_noalloc: max |div B| of a caller-owned device state (device pointer
+    `d_state_ptr`, 8 fields `field_stride` doubles apart) on `stream`, allocating nothing."""
+    lib = load()
+    out = ctypes.c_double()
+    _check(lib.qas_max_divb_noalloc(ctypes.byref(grid), int(odr), ctypes.c_void_p(d_state_ptr),
+                                    int(field_stride), ctypes.c_void_p(stream), ctypes.byref(out)),
+           "qas_max_divb_noalloc")
+    return out.value
