@@ -5,6 +5,9 @@
   ``oracle/Makefile`` with the reference flags -O2 -fopenmp) and reads back
   the state and the dt sequence.
 * ``run_kat``: point-function known answers from ``oracle/_ref/ref_kat``.
+* ``run_reference_dual``: the reference's 2D stepping code built with a
+  forward-mode dual number for double (``oracle/_ref/ref2d_dual_ctw*``): final
+  state and its directional derivative for a given tangent, dt held fixed.
 * ``Restatement``: ctypes binding of ``oracle/liboracle_qas.so``, our plain-C
   restatement of the same algorithm (``oracle/qas_oracle.c``).
 
@@ -95,6 +98,42 @@ def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, 
         subprocess.run([exe, cin, cout], check=True, env=env, timeout=timeout,
                        stdout=subprocess.DEVNULL)
         return read_result(cout, prob)
+
+
+def dual_binary(ctw: int) -> str:
+    return os.path.join(REF_DIR, f"ref2d_dual_ctw{int(bool(ctw))}")
+
+
+def run_reference_dual(prob, state: np.ndarray, tangent: np.ndarray, dts, eta0: float = 0.0, deta: float = 0.0,
+                       nthreads: int = 0, timeout: float = 3600.0):
+    """Tangent-linear run of the reference's 2D code (bound, ideal, sub-cycled dsptv with
+    uniform eta0 and nu = 0 when eta0 > 0) with the given dt per step.  Returns
+    (final state, d(final state)) for the initial tangent (state direction, deta)."""
+    exe = dual_binary(prob.ctw)
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError(f"reference dual binary missing: {exe} (build with `make -C oracle ref`)")
+    if prob.dim != 2:
+        raise ValueError("the dual build covers the 2D driver")
+    st = np.ascontiguousarray(state, dtype=np.float64).reshape(8, -1)
+    tg = np.ascontiguousarray(tangent, dtype=np.float64).reshape(8, -1)
+    d = np.ascontiguousarray(dts, dtype=np.float64)
+    hdr = struct.pack("<10i7d16i", 0x44534151, prob.nxm, prob.nym, prob.rmn, prob.odr, prob.rk, int(bool(prob.ctw)),
+                      d.size, nthreads, 0, prob.gam, prob.xmin, prob.xmax, prob.ymin, prob.ymax, float(eta0),
+                      float(deta), *[int(x) for x in prob.dnx], *[int(x) for x in prob.dny])
+    with tempfile.TemporaryDirectory(prefix="qasdual_") as td:
+        cin = os.path.join(td, "case.bin")
+        cout = os.path.join(td, "result.bin")
+        with open(cin, "wb") as f:
+            f.write(hdr)
+            f.write(d.tobytes())
+            f.write(st.tobytes())
+            f.write(tg.tobytes())
+        env = dict(os.environ)
+        if nthreads > 0:
+            env["OMP_NUM_THREADS"] = str(nthreads)
+        subprocess.run([exe, cin, cout], check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
+        out = np.fromfile(cout, dtype=np.float64).reshape(2, 8, -1)
+    return out[0], out[1]
 
 
 def run_kat(func: int, inputs: np.ndarray, nout: int) -> np.ndarray:
