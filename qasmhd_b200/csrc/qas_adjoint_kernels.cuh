@@ -31,6 +31,7 @@ struct InvMaps {
   const int *idx;
   const double *fac;
   int nmax, kmax;
+  int lo[2][2], hi[2][2];  // per group and axis: indices whose inverse map is the identity for every field
 };
 
 // One reverse stage.  Tape arrays are read-only; adjoint arrays as documented.
@@ -64,42 +65,63 @@ struct AView {
   if (i >= (g).nx || j >= (g).ny) return;              \
   const long long c = (long long)(g).nx * j + i;
 
-// sum over the fill preimage of cell (i,j): the transpose of the ghost fill of
-// group G / field f applied to array a (0 at cells that the fill writes)
+// Sum over the fill preimage of cell (i,j): the transpose of the ghost fill of group G /
+// field f applied to array a (0 at cells that the fill writes).  A 2D preimage has at most
+// ADJ_KMAX indices per axis (the index itself plus the 4 ghosts of an open boundary), checked
+// on the host; the entries are loaded unconditionally (an unused entry points at the cell
+// itself) so that all loads of a boundary cell are in flight together.
+#define ADJ_KMAX 5
+__device__ __forceinline__ void preimage(const InvMaps &im, int G, int f, int ax, int i, int ii[ADJ_KMAX],
+                                         double fa[ADJ_KMAX])
+{
+  const int e = ((G * 8 + f) * 3 + ax) * im.nmax + i;
+  const int n = im.cnt[e];
+#pragma unroll
+  for (int q = 0; q < ADJ_KMAX; q++) {
+    const bool ok = q < n;
+    ii[q] = ok ? im.idx[e * im.kmax + q] : i;
+    fa[q] = ok ? im.fac[e * im.kmax + q] : 0.0;
+  }
+}
 __device__ __forceinline__ double bound_t(const InvMaps &im, const Geo &g, int G, int f, const double *a, int i, int j)
 {
-  const int bxi = ((G * 8 + f) * 3 + 0) * im.nmax + i;
-  const int byi = ((G * 8 + f) * 3 + 1) * im.nmax + j;
-  const int nxq = im.cnt[bxi], nyq = im.cnt[byi];
+  if (i >= im.lo[G][0] && i < im.hi[G][0] && j >= im.lo[G][1] && j < im.hi[G][1]) return a[(long long)g.nx * j + i];
+  int ix[ADJ_KMAX], jy[ADJ_KMAX];
+  double fx[ADJ_KMAX], fy[ADJ_KMAX];
+  preimage(im, G, f, 0, i, ix, fx);
+  preimage(im, G, f, 1, j, jy, fy);
   double s = 0.0;
-  for (int qy = 0; qy < nyq; qy++) {
-    const int jj = im.idx[byi * im.kmax + qy];
-    const double fy = im.fac[byi * im.kmax + qy];
-    for (int qx = 0; qx < nxq; qx++) {
-      const int ii = im.idx[bxi * im.kmax + qx];
-      const double fx = im.fac[bxi * im.kmax + qx];
-      s += (fx * fy) * a[(long long)g.nx * jj + ii];
+#pragma unroll
+  for (int qy = 0; qy < ADJ_KMAX; qy++)
+#pragma unroll
+    for (int qx = 0; qx < ADJ_KMAX; qx++) {
+      const double v = a[(long long)g.nx * jy[qy] + ix[qx]];
+      const double w = fx[qx] * fy[qy];
+      s += (w != 0.0) ? w * v : 0.0;
     }
-  }
   return s;
 }
 __device__ __forceinline__ double bound_t2(const InvMaps &im, const Geo &g, int G, int f, const double *a,
                                            const double *b, int i, int j)
 {
-  const int bxi = ((G * 8 + f) * 3 + 0) * im.nmax + i;
-  const int byi = ((G * 8 + f) * 3 + 1) * im.nmax + j;
-  const int nxq = im.cnt[bxi], nyq = im.cnt[byi];
-  double s = 0.0;
-  for (int qy = 0; qy < nyq; qy++) {
-    const int jj = im.idx[byi * im.kmax + qy];
-    const double fy = im.fac[byi * im.kmax + qy];
-    for (int qx = 0; qx < nxq; qx++) {
-      const int ii = im.idx[bxi * im.kmax + qx];
-      const double fx = im.fac[bxi * im.kmax + qx];
-      const long long p = (long long)g.nx * jj + ii;
-      s += (fx * fy) * (a[p] + b[p]);
-    }
+  if (i >= im.lo[G][0] && i < im.hi[G][0] && j >= im.lo[G][1] && j < im.hi[G][1]) {
+    const long long p = (long long)g.nx * j + i;
+    return a[p] + b[p];
   }
+  int ix[ADJ_KMAX], jy[ADJ_KMAX];
+  double fx[ADJ_KMAX], fy[ADJ_KMAX];
+  preimage(im, G, f, 0, i, ix, fx);
+  preimage(im, G, f, 1, j, jy, fy);
+  double s = 0.0;
+#pragma unroll
+  for (int qy = 0; qy < ADJ_KMAX; qy++)
+#pragma unroll
+    for (int qx = 0; qx < ADJ_KMAX; qx++) {
+      const long long p = (long long)g.nx * jy[qy] + ix[qx];
+      const double v = a[p] + b[p];
+      const double w = fx[qx] * fy[qy];
+      s += (w != 0.0) ? w * v : 0.0;
+    }
   return s;
 }
 
@@ -130,15 +152,21 @@ __device__ __forceinline__ bool upd_region(const Geo &g, int m, int i, int j)
 // ---------------------------------------------------------------------------
 // bound^T + RK combine^T
 // ---------------------------------------------------------------------------
+// (every kernel below issues all of its loads before its first store: the arrays are
+// distinct but the compiler cannot prove it, and interleaving would serialise the loads)
 __global__ void k_a_update(AView a)
 {
   QAS_ADJ_CELL(a.g);
+  double w[8], o[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) w[m] = upd_region(a.g, m, i, j) ? bound_t(a.im, a.g, 0, m, a.ao[m], i, j) : 0.0;
+#pragma unroll
+  for (int m = 0; m < 8; m++) o[m] = a.a0[m][c];
 #pragma unroll
   for (int m = 0; m < 8; m++) {
-    const double w = upd_region(a.g, m, i, j) ? bound_t(a.im, a.g, 0, m, a.ao[m], i, j) : 0.0;
-    a.w[m][c] = w;
-    a.ai[m][c] = a.c1 * w;
-    a.a0[m][c] += a.c0 * w;
+    a.w[m][c] = w[m];
+    a.ai[m][c] = a.c1 * w[m];
+    a.a0[m][c] = o[m] + a.c0 * w[m];
   }
 }
 
@@ -147,8 +175,11 @@ __global__ void k_a_update(AView a)
 __global__ void k_a_fold(AView a)
 {
   QAS_ADJ_CELL(a.g);
+  double r[8];
 #pragma unroll
-  for (int m = 0; m < 8; m++) a.ai[m][c] = bound_t2(a.im, a.g, 0, m, a.ao[m], a.a0[m], i, j);
+  for (int m = 0; m < 8; m++) r[m] = bound_t2(a.im, a.g, 0, m, a.ao[m], a.a0[m], i, j);
+#pragma unroll
+  for (int m = 0; m < 8; m++) a.ai[m][c] = r[m];
 }
 
 // ---------------------------------------------------------------------------
@@ -219,9 +250,8 @@ __global__ void k_a_emf(AView a)
 // face flux adjoint + Roe VJP along axis A
 // ---------------------------------------------------------------------------
 template <int A>
-__global__ void __launch_bounds__(128) k_a_flux(AView a)
+__device__ __forceinline__ void a_flux_cell(const AView &a, int i, int j, long long c)
 {
-  QAS_ADJ_CELL(a.g);
   const Geo &g = a.g;
   const int pos = A == 0 ? i : j;
   const int n = g.n[A];
@@ -278,13 +308,14 @@ __global__ void __launch_bounds__(128) k_a_flux(AView a)
   const double bnf = a.u[4 + A][c];
   const double bn = 0.5 * (bnf + bnf);
   double gbn = 0.0;
+  const double ob = a.ai[4 + A][c];
   flux_roe_vjp(L, R, bn, a.gam, Fb, gL, gR, gbn);
 #pragma unroll
   for (int m = 0; m < 7; m++) {
     a.avl[m][c - s] = gL[m];
     a.avr[m][c] = gR[m];
   }
-  a.ai[4 + A][c] += gbn;
+  a.ai[4 + A][c] = ob + gbn;
   a.aql[c - s] = 0.5 * fcb;
   a.aqr[c] = 0.5 * fcb;
 }
@@ -293,9 +324,8 @@ __global__ void __launch_bounds__(128) k_a_flux(AView a)
 // characteristic reconstruction VJP along axis A -> stencil-slot adjoints
 // ---------------------------------------------------------------------------
 template <int A>
-__global__ void __launch_bounds__(128) k_a_lr(AView a)
+__device__ __forceinline__ void a_lr_cell(const AView &a, int i, int j, long long c)
 {
-  QAS_ADJ_CELL(a.g);
   const Geo &g = a.g;
   const int pos = A == 0 ? i : j;
   const int n = g.n[A];
@@ -310,8 +340,8 @@ __global__ void __launch_bounds__(128) k_a_lr(AView a)
   const double *vt = A == 0 ? vb : vc;
   const bool in = pos >= 2 && pos < n - 2;
   // normal-face B of the induction states: bfr = b[c] for this cell, bfl = b[c] for cell c-s
+  double badd = 0.0;
   {
-    double badd = 0.0;
     if (in) {
       double f[5];
 #pragma unroll
@@ -324,12 +354,13 @@ __global__ void __launch_bounds__(128) k_a_lr(AView a)
       for (int m = 0; m < 5; m++) f[m] = vt[c - s + (m - 2) * s];
       badd += -lin_left<4>(f) * a.aql[c - s];
     }
-    a.ai[4 + A][c] += badd;
   }
   double *gsA = a.gs + (long long)A * 36 * a.ast;
   if (!in) {
+    const double ob = a.ai[4 + A][c];
 #pragma unroll
     for (int q = 0; q < 36; q++) gsA[q * a.ast + c] = 0.0;
+    a.ai[4 + A][c] = ob + badd;
     return;
   }
   double q[7][5], gq[7][5];
@@ -353,6 +384,7 @@ __global__ void __launch_bounds__(128) k_a_lr(AView a)
     gvr[m] = a.avr[m][c];
   }
   double gbn = 0.0;
+  const double ob = a.ai[4 + A][c];
   face_states_vjp(q, cn[c], a.gam, gvl, gvr, gq, gbn);
   // induction states ql = L(bt*vn) - bfl L(vt), qr = R(bt*vn) - bfr R(vt)
   {
@@ -374,6 +406,30 @@ __global__ void __launch_bounds__(128) k_a_lr(AView a)
 #pragma unroll
     for (int m = 0; m < 5; m++) gsA[(v * 5 + m) * a.ast + c] = gq[v][m];
   gsA[35 * a.ast + c] = gbn;
+  a.ai[4 + A][c] = ob + badd;
+}
+
+// The two heavy reverse kernels run persistent: a grid of (SMs x resident blocks) walks
+// 128-cell strips along x, so the last wave is never a few stray blocks (at 256^2 the
+// tiled launch needed 3 waves of which the last held 2 blocks).
+#define QAS_ADJ_STRIPS(body)                                                        \
+  const long long ncell = (long long)a.g.nx * a.g.ny;                              \
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell;  \
+       t += (long long)gridDim.x * blockDim.x) {                                    \
+    const int i = (int)(t % a.g.nx), j = (int)(t / a.g.nx);                         \
+    body;                                                                           \
+  }
+
+template <int A>
+__global__ void __launch_bounds__(128) k_a_flux(AView a)
+{
+  QAS_ADJ_STRIPS(a_flux_cell<A>(a, i, j, t));
+}
+
+template <int A>
+__global__ void __launch_bounds__(128) k_a_lr(AView a)
+{
+  QAS_ADJ_STRIPS(a_lr_cell<A>(a, i, j, t));
 }
 
 // ---------------------------------------------------------------------------
@@ -453,14 +509,17 @@ __global__ void k_a_prim(AView a)
   czb += -gm1 * cz * prb;
   const double irob = a.u[1][c] * vxb + a.u[2][c] * vyb + a.u[3][c] * vzb;
   rob += -iro * iro * irob;
-  a.ai[0][c] += rob;
-  a.ai[1][c] += iro * vxb;
-  a.ai[2][c] += iro * vyb;
-  a.ai[3][c] += iro * vzb;
-  a.ai[4][c] += bxb;
-  a.ai[5][c] += byb;
-  a.ai[6][c] += czb;
-  a.ai[7][c] += enb;
+  double o[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) o[m] = a.ai[m][c];
+  a.ai[0][c] = o[0] + rob;
+  a.ai[1][c] = o[1] + iro * vxb;
+  a.ai[2][c] = o[2] + iro * vyb;
+  a.ai[3][c] = o[3] + iro * vzb;
+  a.ai[4][c] = o[4] + bxb;
+  a.ai[5][c] = o[5] + byb;
+  a.ai[6][c] = o[6] + czb;
+  a.ai[7][c] = o[7] + enb;
   a.acx[c] = cxb;
   a.acy[c] = cyb;
 }
@@ -480,15 +539,17 @@ __global__ void k_a_cb(AView a)
     const int sj = j + 1 - m;
     if (sj >= 0 && sj < g.ny) byb += w[m] * bound_t(a.im, g, 1, 1, a.acy, i, sj);
   }
-  a.ai[4][c] += bxb;
-  a.ai[5][c] += byb;
+  const double ox = a.ai[4][c], oy = a.ai[5][c];
+  a.ai[4][c] = ox + bxb;
+  a.ai[5][c] = oy + byb;
 }
 
 // ---------------------------------------------------------------------------
 // resistive stage of dsptv (nu = 0): E = eta J at the CT edges (mhd_ct_eres),
 // resistive face fluxes (calc_flux_resistive), CT update of bx, by, flux update
 // of bz, en.  Dissipative kernels share k_a_update / k_a_fold.
-// Scratch use: avl[0..3] = flux adjoints (x bz, x en, y bz, y en), avl[4..6] = J adjoint.
+// Scratch use: avl[0..3] = flux adjoints (x bz, x en, y bz, y en), avl[4..6] = J adjoint,
+// avr[0..2] = the forward E.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool dflux_in(const Geo &g, int i, int j)
 {
@@ -570,6 +631,8 @@ __global__ void k_d_emf(AView a, double eta, double idx, double idy)
   if (!dflux_in(g, i, j)) {
 #pragma unroll
     for (int q = 4; q < 7; q++) a.avl[q][c] = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; q++) a.avr[q][c] = 0.0;  // E is not formed outside the eres range
     return;
   }
   const long long sy = g.s[1];
@@ -586,12 +649,17 @@ __global__ void k_d_emf(AView a, double eta, double idx, double idy)
   // ex: y-face bz flux (-ex) and energy flux (-ex bz0)
   const double exb = -a.avl[2][c] - bz0_yface(a, c) * a.avl[3][c];
   const double e4 = 0.25 * (eta + eta + eta + eta);
+  double jx, jy, jz;
+  cur_j(a, c, idx, idy, jx, jy, jz);
+  const double oeb = a.eb[c];
   a.avl[4][c] = e4 * exb;
   a.avl[5][c] = e4 * eyb;
   a.avl[6][c] = e4 * ezb;
-  double jx, jy, jz;
-  cur_j(a, c, idx, idy, jx, jy, jz);
-  a.eb[c] += jx * exb + jy * eyb + jz * ezb;
+  a.eb[c] = oeb + (jx * exb + jy * eyb + jz * ezb);
+  // the forward E of this cell (mhd_ct_eres), for k_d_b
+  a.avr[0][c] = e4 * jx;
+  a.avr[1][c] = e4 * jy;
+  a.avr[2][c] = e4 * jz;
 }
 
 __global__ void k_d_b(AView a, double eta, double idx, double idy)
@@ -601,7 +669,6 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
   const long long sy = g.s[1];
   const double dw[4] = {1.0 / 24.0, -27.0 / 24.0, 27.0 / 24.0, -1.0 / 24.0};  // dfc<4> weights of fm, f0, f1, f2
   const double cw[4] = {-0.0625, 0.5625, 0.5625, -0.0625};                     // fcen<4> weights
-  const double e4 = 0.25 * (eta + eta + eta + eta);
   const double *jxb = a.avl[4], *jyb = a.avl[5], *jzb = a.avl[6];
   double bxb = 0.0, byb = 0.0, bzb = 0.0;
   // J^T: point m of the stencil at cell c is c + (m-2) s for m = 0..3
@@ -623,7 +690,9 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
   }
   // energy fluxes: x face f: ey[f] bz0 - 0.5 (ez[f] + ez[f+sy]) by0
   //                y face f: 0.5 (ez[f] + ez[f+1]) bx0 - ex[f] bz0
-  double jx, jy, jz;
+  // (E from k_d_emf: zero outside the eres range, as the forward never reads it there
+  //  for a face whose flux adjoint is non-zero)
+  const double *ex = a.avr[0], *ey = a.avr[1], *ez = a.avr[2];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
     // bz[c] is point m of the x face f = c - (m-2)
@@ -631,8 +700,7 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
       const int fi = i - (m - 2);
       if (fi >= 0 && fi < g.nx && dflux_in(g, fi, j)) {
         const long long f = c - (m - 2);
-        cur_j(a, f, idx, idy, jx, jy, jz);
-        bzb += (e4 * jy) * cw[m] * a.avl[1][f];
+        bzb += ey[f] * cw[m] * a.avl[1][f];
       }
     }
     // by[c] is point m of x face f = c - (m-2) (as p) and of f = c - sy - (m-2) (as p + sy)
@@ -641,10 +709,7 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
       const int fi = i - (m - 2), fj = j - h;
       if (fi >= 0 && fi < g.nx && fj >= 0 && dflux_in(g, fi, fj)) {
         const long long f = c - (m - 2) - h * sy;
-        double jx1 = 0.0, jy1 = 0.0, jz1 = 0.0;  // E is not formed beyond the eres range
-        cur_j(a, f, idx, idy, jx, jy, jz);
-        if (dflux_in(g, fi, fj + 1)) cur_j(a, f + sy, idx, idy, jx1, jy1, jz1);
-        const double ez0 = 0.5 * (e4 * jz + e4 * jz1);
+        const double ez0 = 0.5 * (ez[f] + ez[f + sy]);
         byb += -ez0 * 0.5 * cw[m] * a.avl[1][f];
       }
     }
@@ -654,10 +719,7 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
       const int fi = i - h, fj = j - (m - 2);
       if (fj >= 0 && fj < g.ny && fi >= 0 && dflux_in(g, fi, fj)) {
         const long long f = c - (m - 2) * sy - h;
-        double jx1 = 0.0, jy1 = 0.0, jz1 = 0.0;
-        cur_j(a, f, idx, idy, jx, jy, jz);
-        if (dflux_in(g, fi + 1, fj)) cur_j(a, f + 1, idx, idy, jx1, jy1, jz1);
-        const double ey0 = 0.5 * (e4 * jz + e4 * jz1);
+        const double ey0 = 0.5 * (ez[f] + ez[f + 1]);
         bxb += ey0 * 0.5 * cw[m] * a.avl[3][f];
       }
     }
@@ -666,14 +728,14 @@ __global__ void k_d_b(AView a, double eta, double idx, double idy)
       const int fj = j - (m - 2);
       if (fj >= 0 && fj < g.ny && dflux_in(g, i, fj)) {
         const long long f = c - (m - 2) * sy;
-        cur_j(a, f, idx, idy, jx, jy, jz);
-        bzb += -(e4 * jx) * cw[m] * a.avl[3][f];
+        bzb += -ex[f] * cw[m] * a.avl[3][f];
       }
     }
   }
-  a.ai[4][c] += bxb;
-  a.ai[5][c] += byb;
-  a.ai[6][c] += bzb;
+  const double ox = a.ai[4][c], oy = a.ai[5][c], oz = a.ai[6][c];
+  a.ai[4][c] = ox + bxb;
+  a.ai[5][c] = oy + byb;
+  a.ai[6][c] = oz + bzb;
 }
 
 // deterministic sum of the per-cell eta adjoint (one block)

@@ -191,24 +191,32 @@ __global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
   const long long sy = g.s[1];
   const double dtdx = dc->sdtd[0], dtdy = dc->sdtd[1];
   const bool ci = i < g.nx - GH, cj = j < g.ny - GH;
+  // all new values before the first store (see update_body)
+  const int cen[6] = {0, 1, 2, 3, 6, 7};
+  double nv[6], nbx = 0.0, nby = 0.0;
   if (ci && cj) {
-    const int cen[6] = {0, 1, 2, 3, 6, 7};
 #pragma unroll
     for (int q = 0; q < 6; q++) {
       const int m = cen[q];
       const double du0 = d4<ODR>(v.f[0][m], c, 1);
       const double du1 = d4<ODR>(v.f[1][m], c, sy);
-      v.u[m][c] = rk_combine(v.u[m][c], v.u0[m][c], (-dtdx * du0 - dtdy * du1), c0, c1);
+      nv[q] = rk_combine(v.u[m][c], v.u0[m][c], (-dtdx * du0 - dtdy * du1), c0, c1);
     }
   }
   if (cj) {
     const double du = d4<ODR>(v.ez, c, sy);
-    v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+    nbx = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
   }
   if (ci) {
     const double du = d4<ODR>(v.ez, c, 1);
-    v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+    nby = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
   }
+  if (ci && cj) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) v.u[cen[q]][c] = nv[q];
+  }
+  if (cj) v.u[4][c] = nbx;
+  if (ci) v.u[5][c] = nby;
 }
 
 __global__ void k_dbound(View v, const DCtl *dc, int nc)
@@ -218,18 +226,7 @@ __global__ void k_dbound(View v, const DCtl *dc, int nc)
   if (t >= shell_cells(v.g)) return;
   int i, j, k;
   shell_cell(v.g, t, i, j, k);
-  const Geo &g = v.g;
-  const long long c = cidx(g, i, j, k);
-#pragma unroll
-  for (int m = 0; m < 8; m++) {
-    int si, sj, sk;
-    double fac;
-    gather_src(v, 0, m, i, j, k, si, sj, sk, fac);
-    if (si != i || sj != j || sk != k) {
-      double *u = v.u[m];
-      u[c] = fac * u[cidx(g, si, sj, sk)];
-    }
-  }
+  bound_body(v, i, j, k);
 }
 
 // ut = u at the start of each dsptv call

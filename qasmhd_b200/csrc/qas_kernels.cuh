@@ -600,6 +600,12 @@ __device__ __forceinline__ void update_body(const View &v, int i, int j, int k, 
   const bool cj = g.dim < 2 || j < g.ny - GH;
   const bool ck = g.dim < 3 || k < g.nz - GH;
   const long long sy = g.s[1], sz = g.s[2];
+  // every new value is formed before the first store (the compiler cannot prove that the
+  // state and flux arrays do not alias, and interleaved stores would serialise the loads)
+  double nv[8];
+  bool wr[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) wr[m] = false;
   if (ci && cj && ck) {
 #pragma unroll
     for (int m = 0; m < 8; m++) {
@@ -619,35 +625,44 @@ __device__ __forceinline__ void update_body(const View &v, int i, int j, int k, 
           du = (-dtdx * du0 - dtdy * du1 - dtdz * du2);
         }
       }
-      v.u[m][c] = rk_combine(v.u[m][c], v.u0[m][c], du, c0, c1);
+      nv[m] = rk_combine(v.u[m][c], v.u0[m][c], du, c0, c1);
+      wr[m] = true;
     }
   }
   if (g.dim == 2) {
     if (cj) {  // bx on i in [GH, nx-GH]
       const double du = d4<ODR>(v.ez, c, sy);
-      v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+      nv[4] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+      wr[4] = true;
     }
     if (ci && j <= g.ny - GH) {  // by on j in [GH, ny-GH]
       const double du = d4<ODR>(v.ez, c, 1);
-      v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+      nv[5] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+      wr[5] = true;
     }
   } else if (g.dim == 3) {
     if (ck && cj) {
       const double du0 = +d4<ODR>(v.ez, c, sy);
       const double du1 = -d4<ODR>(v.ey, c, sz);
-      v.u[4][c] = rk_combine(v.u[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
+      nv[4] = rk_combine(v.u[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
+      wr[4] = true;
     }
     if (ck && ci) {
       const double du0 = +d4<ODR>(v.ex, c, sz);
       const double du1 = -d4<ODR>(v.ez, c, 1);
-      v.u[5][c] = rk_combine(v.u[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
+      nv[5] = rk_combine(v.u[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
+      wr[5] = true;
     }
     if (cj && ci) {
       const double du0 = +d4<ODR>(v.ey, c, 1);
       const double du1 = -d4<ODR>(v.ex, c, sy);
-      v.u[6][c] = rk_combine(v.u[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
+      nv[6] = rk_combine(v.u[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
+      wr[6] = true;
     }
   }
+#pragma unroll
+  for (int m = 0; m < 8; m++)
+    if (wr[m]) v.u[m][c] = nv[m];
 }
 
 // offset of the update launch: threads start at the first interior cell
@@ -727,16 +742,20 @@ __device__ __forceinline__ void bound_body(const View &v, int i, int j, int k)
 {
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
+  // sources are never written by the fill, so all values are gathered before any store
+  double nv[8];
+  bool wr[8];
 #pragma unroll
   for (int m = 0; m < 8; m++) {
     int si, sj, sk;
     double fac;
     gather_src(v, 0, m, i, j, k, si, sj, sk, fac);
-    if (si != i || sj != j || sk != k) {
-      double *u = v.u[m];
-      u[c] = fac * u[cidx(g, si, sj, sk)];
-    }
+    wr[m] = si != i || sj != j || sk != k;
+    nv[m] = wr[m] ? fac * v.u[m][cidx(g, si, sj, sk)] : 0.0;
   }
+#pragma unroll
+  for (int m = 0; m < 8; m++)
+    if (wr[m]) v.u[m][c] = nv[m];
 }
 
 __global__ void k_bound(View v)
