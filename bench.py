@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="print only the adjoint comparison over --steps steps (profiling aid)")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="print only the batched-ensemble comparison over --steps steps (profiling aid)")
     return ap.parse_args()
 
 
@@ -231,8 +235,8 @@ def adjoint_compare(nsteps=400, every=20, eta=0.5e-4):
             "forward_ms_per_step": ms_f / nsteps, "adjoint_forward_ms_per_step": ms_af / nsteps,
             "backward_ms_per_step": ms_b / nsteps, "ratio": ms_b / ms_f,
             "ratio_with_checkpointed_forward": (ms_af + ms_b) / ms_f,
-            "basis": "ratio = backward (segment recompute with tape + reverse sweep) / plain forward of the "
-                     "same 400 steps; gradients checked against the reference's dual-number derivative"}
+            "basis": f"ratio = backward (segment recompute with tape + reverse sweep) / plain forward of the "
+                     f"same {nsteps} steps; gradients checked against the reference's dual-number derivative"}
 
 
 def run_reference_arm(args):
@@ -274,6 +278,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.adjoint_only or args.ensemble_only:
+        if rank == 0:
+            out = {}
+            if args.adjoint_only:
+                out["adjoint"] = adjoint_compare(nsteps=args.steps)
+            if args.ensemble_only:
+                out["batched"] = ensemble_compare(args.steps)
+            print(json.dumps(out))
+        return
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
