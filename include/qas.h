@@ -40,7 +40,8 @@ typedef enum {
   QAS_ERR_NONFINITE = 4,    /* device check found rho<=0, p<=0 or a non-finite value */
   QAS_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up                    */
   QAS_ERR_UNSUPPORTED = 6,  /* combination not implemented                           */
-  QAS_ERR_NO_DEVICE = 7     /* no usable CUDA device                                 */
+  QAS_ERR_NO_DEVICE = 7,    /* no usable CUDA device                                 */
+  QAS_ERR_IO = 8            /* a file could not be written or read (message: qas_last_cuda_error) */
 } qas_status;
 
 /* Grid: compile-time XMESH/YMESH/ZMESH of mymacros.hpp plus paras()'s spacing and gamma
@@ -227,6 +228,27 @@ qas_status qas_batch_set_tile(qas_batch *batch, const char *kernel, int tx, int 
 qas_status qas_batch_autotune(qas_batch *batch, int trial_steps);
 qas_status qas_batch_stream(qas_batch *batch, void **stream);
 qas_status qas_batch_kernel_launches(const qas_batch *batch, long long *count);
+
+/* ------------------------------------------------------------------------------------
+ * The reference's on-disk formats for the context's state.
+ * qas_dout: dout_() of MHD1D (1D/SERIAL/shock/mhd1d_class.cpp:57-95), MHD2D
+ * (2D/SERIAL/OTvortex/mhd2d_class.cpp:63-114) and single-rank MHD3D
+ * (3D/MPI/KHI/mhd3d_class.cpp:78-145) into directory `dir`: with n == 0 the header files
+ * (params, offsets/xoff, mpinum in 3D, t, coordinates x_i = (i - 4 + 0.5) dx + origin[0] ...),
+ * otherwise t.dat is appended; then outdat_<cnt>.dat (3D: outdat_<cnt>_00000.dat as float).
+ * Asynchronous: the state is snapshot in the context's stream order and written by a host
+ * thread while the caller keeps stepping; qas_dout_wait joins it and returns its status (a
+ * new qas_dout first waits for the previous one).
+ * qas_bkup_save / qas_bkup_load: bkup_save / bkup_load (common/common_func.c:280-344):
+ * bkup_stamp.dat ("n cnt"), bkup_time.dat (tim, dt, trec), bkup_data_<rank>.dat.  As in the
+ * reference, a missing stamp file is not an error: *loaded = 0 and nothing changes.
+ * ------------------------------------------------------------------------------------ */
+qas_status qas_dout(qas_ctx *ctx, const char *dir, int n, int cnt, double tim, const double *const coord[3]);
+qas_status qas_dout_wait(qas_ctx *ctx);
+qas_status qas_bkup_save(qas_ctx *ctx, const char *dir, int n, int cnt, double tim, double dt, double trec,
+                         int rank);
+qas_status qas_bkup_load(qas_ctx *ctx, const char *dir, int rank, int *loaded, int *n, int *cnt, double *tim,
+                         double *dt, double *trec);
 
 /* ------------------------------------------------------------------------------------
  * Discrete adjoint of the 2D step (no counterpart in the reference, which has no

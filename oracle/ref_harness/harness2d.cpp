@@ -110,6 +110,23 @@ class RefHarness2D : public DMHD2D {
     *elapsed = omp_get_wtime() - t0;
     return steps;
   }
+  /* the reference's own writers / reader on this state (I/O pins) */
+  void io(const RefCaseHeader &h, const char *dir)
+  {
+    snprintf(fildir, sizeof(fildir), "%s", dir);
+    if (h.mode == REF_MODE_IO) {
+      n = h.nsteps;
+      cnt = h.flg;
+      tim = h.dt;
+      dt = h.cfl;
+      trec = h.dtrec;
+      dout_(0);
+      bkup_save(val, nm, nd, n, cnt, tim, dt, trec, 0, fildir);
+    } else {
+      bkup_load(val, nm, nd, &n, &cnt, &tim, &dt, &trec, 0, fildir);
+      ref_write_loaded(dir, n, cnt, tim, dt, trec);
+    }
+  }
   double time_now() const { return tim; }
   double dt_now() const { return dt; }
   double *const *state() const { return val; }
@@ -118,7 +135,7 @@ class RefHarness2D : public DMHD2D {
 
 int main(int argc, char **argv)
 {
-  if (argc != 3) ref_die("usage: ref2d <case.bin> <result.bin>");
+  if (argc != 3 && argc != 4) ref_die("usage: ref2d <case.bin> <result.bin> [io dir]");
   RefCaseHeader h;
   std::vector<double> data;
   ref_read_case(argv[1], &h, &data);
@@ -134,7 +151,13 @@ int main(int argc, char **argv)
   sim->setup(h, data.data());
   std::vector<double> dts;
   double elapsed = 0.0;
-  int steps = sim->run(h, &dts, &elapsed);
+  int steps = 0;
+  if (h.mode == REF_MODE_IO || h.mode == REF_MODE_IOLOAD) {
+    if (argc != 4) ref_die("I/O modes need the directory argument");
+    sim->io(h, argv[3]);
+  } else {
+    steps = sim->run(h, &dts, &elapsed);
+  }
 
   RefResultHeader r;
   memset(&r, 0, sizeof(r));

@@ -25,8 +25,13 @@ enum RefMode {
   REF_MODE_RUN  = 1,   /* setdt(1); nsteps x { tim+=dt; bound; ideal; setdt(flg) } */
   REF_MODE_EXEC = 2,   /* exec_(flg) loop termination: n<nmax && tim<tmax          */
   REF_MODE_DRUN = 3,   /* RUN with the dissipative sub-cycle after ideal (2D only) */
-  REF_MODE_DSTEP = 4   /* bound; dsptv(dt) once (2D only)                          */
+  REF_MODE_DSTEP = 4,  /* bound; dsptv(dt) once (2D only)                          */
+  REF_MODE_IO = 5,     /* dout_ + bkup_save of the state into argv[3] (n = nsteps,
+                          cnt = flg, tim = dt, dt = cfl, trec = dtrec)             */
+  REF_MODE_IOLOAD = 6  /* bkup_load from argv[3]; the loaded counters go to
+                          argv[3]/loaded.txt, the loaded state to the result       */
 };
+
 
 #pragma pack(push, 1)
 struct RefCaseHeader {
@@ -50,6 +55,17 @@ static inline void ref_die(const char *msg)
 {
   fprintf(stderr, "qas ref harness: %s\n", msg);
   exit(2);
+}
+
+/* Counters of a bkup_load, for the I/O pins. */
+static inline void ref_write_loaded(const char *dir, int n, int cnt, double tim, double dt, double trec)
+{
+  char path[512];
+  snprintf(path, sizeof(path), "%s/loaded.txt", dir);
+  FILE *f = fopen(path, "w");
+  if (!f) ref_die("cannot write loaded.txt");
+  fprintf(f, "%d %d %.17g %.17g %.17g\n", n, cnt, tim, dt, trec);
+  fclose(f);
 }
 
 static inline void ref_read_case(const char *path, RefCaseHeader *h, std::vector<double> *data)

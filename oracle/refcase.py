@@ -29,7 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIB_PATH = os.path.join(HERE, "liboracle_qas.so")
 
-MODE_STEP, MODE_RUN, MODE_EXEC, MODE_DRUN, MODE_DSTEP = 0, 1, 2, 3, 4
+MODE_STEP, MODE_RUN, MODE_EXEC, MODE_DRUN, MODE_DSTEP, MODE_IO, MODE_IOLOAD = 0, 1, 2, 3, 4, 5, 6
 
 _HDR = struct.Struct("<15i12d24i")
 _RES = struct.Struct("<4i4d")
@@ -98,6 +98,33 @@ def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, 
         subprocess.run([exe, cin, cout], check=True, env=env, timeout=timeout,
                        stdout=subprocess.DEVNULL)
         return read_result(cout, prob)
+
+
+def reference_io(prob, directory: str, state: Optional[np.ndarray] = None, load: bool = False, n: int = 0,
+                 cnt: int = 0, tim: float = 0.0, dt: float = 0.0, trec: float = 0.0):
+    """The reference's own dout_ + bkup_save of `state` into `directory` (load=False), or its
+    bkup_load from there (load=True: returns (state, (n, cnt, tim, dt, trec)))."""
+    exe = ref_binary(prob.dim, prob.ctw)
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError(f"reference oracle binary missing: {exe}")
+    import copy
+    p = copy.copy(prob)
+    p.cfl, p.dtrec = float(dt), float(trec)
+    with tempfile.TemporaryDirectory(prefix="qasrefio_") as td:
+        cin = os.path.join(td, "case.bin")
+        cout = os.path.join(td, "result.bin")
+        write_case(cin, p, MODE_IOLOAD if load else MODE_IO, nsteps=int(n), dt=float(tim), state=state)
+        # cnt travels in the flg field
+        raw = bytearray(open(cin, "rb").read())
+        struct.pack_into("<i", raw, 4 * 11, int(cnt))
+        open(cin, "wb").write(bytes(raw))
+        subprocess.run([exe, cin, cout, directory], check=True, stdout=subprocess.DEVNULL)
+        res = read_result(cout, prob)
+    if not load:
+        return None
+    with open(os.path.join(directory, "loaded.txt")) as f:
+        t = f.read().split()
+    return res["state"], (int(t[0]), int(t[1]), float(t[2]), float(t[3]), float(t[4]))
 
 
 def dual_binary(ctw: int) -> str:

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdarg>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -45,6 +46,8 @@ double hmin(double a, double b) { return (a >= b) ? b : a; }  // common/common_f
 
 struct AdjState;  // discrete-adjoint run state (qas_adjoint_api.inc)
 static void adj_free(qas_ctx *c);
+struct IoState;  // asynchronous output writer (qas_io.inc)
+static void io_free(qas_ctx *c);
 
 struct qas_ctx {
   int device = 0;
@@ -87,6 +90,7 @@ struct qas_ctx {
   double prof_ms[32] = {0};
   long long prof_n[32] = {0};
   AdjState *adj = nullptr;
+  IoState *io = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -469,6 +473,7 @@ const char *qas_status_str(qas_status s)
     case QAS_ERR_TIMEOUT: return "bounded device wait timed out";
     case QAS_ERR_UNSUPPORTED: return "unsupported configuration";
     case QAS_ERR_NO_DEVICE: return "no CUDA device";
+    case QAS_ERR_IO: return "file I/O failed";
   }
   return "unknown status";
 }
@@ -592,6 +597,7 @@ qas_status qas_destroy(qas_ctx *c)
   if (!c) return QAS_ERR_INVALID;
   if (c->stream) cudaStreamSynchronize(c->stream);
   adj_free(c);
+  io_free(c);
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
   if (c->pool) cudaFree(c->pool);
@@ -1170,3 +1176,4 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 #include "qas_batch_api.inc"
 #include "qas_adjoint_api.inc"
 #include "qas_noalloc.inc"
+#include "qas_io.inc"

@@ -24,6 +24,7 @@ QAS_ERR_NONFINITE = 4
 QAS_ERR_TIMEOUT = 5
 QAS_ERR_UNSUPPORTED = 6
 QAS_ERR_NO_DEVICE = 7
+QAS_ERR_IO = 8
 
 # every exported entry point of include/qas.h (checked by the CPU tests)
 EXPORTS = (
@@ -35,7 +36,8 @@ EXPORTS = (
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
     "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
-    "qas_adjoint_backward", "qas_max_divb_noalloc",
+    "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
+    "qas_bkup_load",
 )
 QAS_OPT_FUSED_SWEEP = 1
 
@@ -140,6 +142,13 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_fp64_peak.argtypes = [dp]
     lib.qas_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double]
     lib.qas_adjoint_backward.argtypes = [vp, dp, dp, dp]
+    lib.qas_dout.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                             ctypes.POINTER(dp)]
+    lib.qas_dout_wait.argtypes = [vp]
+    lib.qas_bkup_save.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.qas_bkup_load.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ip, ip, ip, dp, dp, dp]
     lib.qas_max_divb_noalloc.argtypes = [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
                                          ctypes.c_void_p, dp]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -154,7 +163,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
 def _check(status: int, what: str) -> None:
     if status != QAS_OK:
         detail = ""
-        if status in (QAS_ERR_CUDA, QAS_ERR_NOMEM) and _lib is not None:
+        if status in (QAS_ERR_CUDA, QAS_ERR_NOMEM, QAS_ERR_IO) and _lib is not None:
             detail = _lib.qas_last_cuda_error().decode()
         raise QasError(status, what, detail)
 
@@ -293,6 +302,37 @@ class Context:
 
     def dsptv(self, dt: float, nu0: float, eta0: float) -> None:
         _check(self.lib.qas_dsptv(self.h, float(dt), float(nu0), float(eta0)), "qas_dsptv")
+
+    # the reference's files ----------------------------------------------------
+    def dout(self, directory: str, n: int, cnt: int, tim: float, coords=None) -> None:
+        """dout_(): header files when n == 0 (`coords` = the x[, y[, z]] cell-centre coordinate
+        arrays over the padded extents), t.dat appended otherwise, then outdat_<cnt>;
+        asynchronous (dout_wait joins the writer)."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        arr = None
+        keep = []
+        if coords is not None:  # copied by the call itself
+            keep = [np.ascontiguousarray(c, dtype=np.float64) for c in coords]
+            arr = (dp * 3)(*([k.ctypes.data_as(dp) for k in keep] + [None] * (3 - len(keep))))
+        _check(self.lib.qas_dout(self.h, directory.encode(), int(n), int(cnt), float(tim), arr), "qas_dout")
+
+    def dout_wait(self) -> None:
+        _check(self.lib.qas_dout_wait(self.h), "qas_dout_wait")
+
+    def bkup_save(self, directory: str, n: int, cnt: int, tim: float, dt: float, trec: float, rank: int = 0) -> None:
+        _check(self.lib.qas_bkup_save(self.h, directory.encode(), int(n), int(cnt), float(tim), float(dt),
+                                      float(trec), int(rank)), "qas_bkup_save")
+
+    def bkup_load(self, directory: str, rank: int = 0):
+        """Returns None when there is no stamp file, else (n, cnt, tim, dt, trec) with the state uploaded."""
+        ld, n, cnt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        tim, dt, trec = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.qas_bkup_load(self.h, directory.encode(), int(rank), ctypes.byref(ld), ctypes.byref(n),
+                                      ctypes.byref(cnt), ctypes.byref(tim), ctypes.byref(dt), ctypes.byref(trec)),
+               "qas_bkup_load")
+        if not ld.value:
+            return None
+        return n.value, cnt.value, tim.value, dt.value, trec.value
 
     # discrete adjoint ---------------------------------------------------------
     def adjoint_forward(self, dts: Sequence[float], eta0: float = 0.0, ckpt_every: int = 20) -> None:
