@@ -81,7 +81,8 @@ typedef struct {
   int nout;          /* N_OUT macro; tmax = dtrec*nout                                           */
   int use_graph;     /* capture the step loop in a CUDA graph                                    */
   double nu0, eta0;  /* uniform viscosity / resistivity: when max(2nu0,eta0) > 1e-15 each step is
-                        followed by the sub-cycled dissipative update of DMHD2D::exec_ (2D only) */
+                        followed by the sub-cycled dissipative update of DMHD2D::exec_ /
+                        DMHD3D::exec_ (2D and 3D) */
 } qas_run_opts;
 
 typedef struct {
@@ -145,8 +146,10 @@ qas_status qas_run(qas_ctx *ctx, const qas_run_opts *opts, qas_run_info *info);
 qas_status qas_run_reset(qas_ctx *ctx);
 
 /* Visco-resistive update with uniform coefficients: DMHD2D::setdc + the sub-cycled
- * dsptv of DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26, dmhd2d_solve.cpp:3-151).
- * qas_dsptv is one dsptv(dt) call (no ghost fill before).  2D only. */
+ * dsptv of DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26, dmhd2d_solve.cpp:3-151),
+ * and of DMHD3D::exec_ (3D/MPI/MRX/dmhd3d_class.cpp:20-28, dmhd3d_solve.cpp:3-179) in 3D.
+ * qas_dsptv is one dsptv(dt) call (no ghost fill before).  2D and 3D (QAS_ERR_UNSUPPORTED
+ * in 1D, which has no dissipative driver in the reference). */
 qas_status qas_dissipate(qas_ctx *ctx, double dt, double nu0, double eta0);
 qas_status qas_dsptv(qas_ctx *ctx, double dt, double nu0, double eta0);
 

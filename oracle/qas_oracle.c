@@ -1405,7 +1405,8 @@ double qo_cfl_dt(const qo_grid *g, const double *u, double unused)
 }
 
 /* ------------------------------------------------------------------------ */
-/* visco-resistive step (2D): 2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151           */
+/* visco-resistive step: 2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151 (2D),          */
+/* 3D/MPI/MRX/dmhd3d_solve.cpp:3-179 (3D)                                      */
 /* ------------------------------------------------------------------------ */
 
 /* eta*J on the CT edges: common/mhd_func.c:78-106 with zoffset = 0 */
@@ -1414,6 +1415,27 @@ static void ct_eres2(const geo *e, const double *bx, const double *by, const dou
 {
   long xo = 1, yo = e->sy, zo = 0;
   double idz = 0.0;
+  long si[4] = {-2 * xo, -xo, 0, +xo}, sj[4] = {-2 * yo, -yo, 0, +yo}, sk[4] = {-2 * zo, -zo, 0, +zo};
+  double bxj[4] = {bx[ss + sj[0]], bx[ss + sj[1]], bx[ss + sj[2]], bx[ss + sj[3]]};
+  double bxk[4] = {bx[ss + sk[0]], bx[ss + sk[1]], bx[ss + sk[2]], bx[ss + sk[3]]};
+  double byk[4] = {by[ss + sk[0]], by[ss + sk[1]], by[ss + sk[2]], by[ss + sk[3]]};
+  double byi[4] = {by[ss + si[0]], by[ss + si[1]], by[ss + si[2]], by[ss + si[3]]};
+  double bzi[4] = {bz[ss + si[0]], bz[ss + si[1]], bz[ss + si[2]], bz[ss + si[3]]};
+  double bzj[4] = {bz[ss + sj[0]], bz[ss + sj[1]], bz[ss + sj[2]], bz[ss + sj[3]]};
+  double jx = df(&bzj[1]) * idy - df(&byk[1]) * idz;
+  double jy = df(&bxk[1]) * idz - df(&bzi[1]) * idx;
+  double jz = df(&byi[1]) * idx - df(&bxj[1]) * idy;
+  const double *et = eta + ss;
+  *ex = 0.25 * (et[-yo - zo] + et[-zo] + et[-yo] + et[0]) * jx;
+  *ey = 0.25 * (et[-zo - xo] + et[-xo] + et[-zo] + et[0]) * jy;
+  *ez = 0.25 * (et[-xo - yo] + et[-yo] + et[-xo] + et[0]) * jz;
+}
+
+/* eta*J on the CT edges in 3D: common/mhd_func.c:78-106 with zoffset = nx*ny */
+static void ct_eres3(const geo *e, const double *bx, const double *by, const double *bz, const double *eta,
+                     double idx, double idy, double idz, pt_fn df, long ss, double *ex, double *ey, double *ez)
+{
+  long xo = 1, yo = e->sy, zo = e->sz;
   long si[4] = {-2 * xo, -xo, 0, +xo}, sj[4] = {-2 * yo, -yo, 0, +yo}, sk[4] = {-2 * zo, -zo, 0, +zo};
   double bxj[4] = {bx[ss + sj[0]], bx[ss + sj[1]], bx[ss + sj[2]], bx[ss + sj[3]]};
   double bxk[4] = {bx[ss + sk[0]], bx[ss + sk[1]], bx[ss + sk[2]], bx[ss + sk[3]]};
@@ -1474,8 +1496,11 @@ static void resist_flux(const double *by, const double *bz, const double *ey, co
   *fen = ey0 * bz0 - ez0 * by0;
 }
 
+static int qo_dsptv3(const qo_grid *g, double *u, double dt, double nu0, double eta0);
+
 int qo_dsptv(const qo_grid *g, double *u, double dt, double nu0, double eta0)
 {
+  if (g->dim == 3) return qo_dsptv3(g, u, dt, nu0, eta0);
   if (g->dim != 2) return -1;
   geo e = mkgeo(g);
   long nd = e.nd, sy = e.sy;
@@ -1564,11 +1589,126 @@ int qo_dsptv(const qo_grid *g, double *u, double dt, double nu0, double eta0)
   return 0;
 }
 
+/* 3D: DMHD3D::dsptv (3D/MPI/MRX/dmhd3d_solve.cpp:3-179) */
+static int qo_dsptv3(const qo_grid *g, double *u, double dt, double nu0, double eta0)
+{
+  geo e = mkgeo(g);
+  long nd = e.nd, sy = e.sy, sz = e.sz;
+  int nx = e.nx, ny = e.ny, nz = e.nz, i, j, k;
+  long ss;
+  double *ut = xcalloc(8 * nd), *fx = xcalloc(8 * nd), *fy = xcalloc(8 * nd), *fz = xcalloc(8 * nd);
+  double *ex = xcalloc(nd), *ey = xcalloc(nd), *ez = xcalloc(nd);
+  double *vx = xcalloc(nd), *vy = xcalloc(nd), *vz = xcalloc(nd), *nu = xcalloc(nd), *eta = xcalloc(nd);
+  if (!ut || !fx || !fy || !fz || !ex || !ey || !ez || !vx || !vy || !vz || !nu || !eta) return -1;
+  for (ss = 0; ss < nd; ss++) { nu[ss] = nu0; eta[ss] = eta0; }
+  pt_fn fc = face_to_centre(g->odr), df = first_diff(g->odr);
+  double idx = 1.0 / g->dx, idy = 1.0 / g->dy, idz = 1.0 / g->dz;
+  double dtdx = dt * idx, dtdy = dt * idy, dtdz = dt * idz;
+  double *f[8];
+  for (int m = 0; m < 8; m++) f[m] = u + (long)m * nd;
+  memcpy(ut, u, sizeof(double) * 8 * nd);
+  for (int rk = 0; rk < g->rk; rk++) {
+    const double *rkf = RKF[g->rk - 1][rk];
+    for (ss = 0; ss < nd; ss++) {
+      double iro = 1.0 / f[0][ss];
+      vx[ss] = f[1][ss] * iro; vy[ss] = f[2][ss] * iro; vz[ss] = f[3][ss] * iro;
+    }
+#pragma omp parallel for collapse(2) schedule(static) private(i, ss)
+    for (k = 2; k < nz - 1; k++)
+      for (j = 2; j < ny - 1; j++)
+        for (i = 2; i < nx - 1; i++) {
+          ss = IDX(e, i, j, k);
+          ct_eres3(&e, f[4], f[5], f[6], eta, idx, idy, idz, df, ss, &ex[ss], &ey[ss], &ez[ss]);
+        }
+#pragma omp parallel for collapse(2) schedule(static) private(i, ss)
+    for (k = 2; k < nz - 1; k++)
+      for (j = 2; j < ny - 1; j++)
+        for (i = 2; i < nx - 1; i++) {
+          ss = IDX(e, i, j, k);
+          double rnu, fl[2][8];
+          memset(fl, 0, sizeof(fl));
+          rnu = 0.5 * (f[0][ss - 1] * nu[ss - 1] + f[0][ss] * nu[ss]);
+          visc_flux(vx, vy, vz, ss, rnu, idx, idy, idz, 1, sy, sz, fc, df, &fl[0][1], &fl[0][2], &fl[0][3], &fl[0][7]);
+          resist_flux(f[5], f[6], ey, ez, ss, 1, sy, sz, fc, &fl[1][5], &fl[1][6], &fl[1][7]);
+          fx[0 * nd + ss] = fl[0][0] + fl[1][0];
+          fx[1 * nd + ss] = fl[0][1] + fl[1][1];
+          fx[2 * nd + ss] = fl[0][2] + fl[1][2];
+          fx[3 * nd + ss] = fl[0][3] + fl[1][3];
+          fx[4 * nd + ss] = 0;
+          fx[5 * nd + ss] = fl[0][5] + fl[1][5];
+          fx[6 * nd + ss] = fl[0][6] + fl[1][6];
+          fx[7 * nd + ss] = fl[0][7] + fl[1][7];
+          rnu = 0.5 * (f[0][ss - sy] * nu[ss - sy] + f[0][ss] * nu[ss]);
+          visc_flux(vy, vz, vx, ss, rnu, idy, idz, idx, sy, sz, 1, fc, df, &fl[0][1], &fl[0][2], &fl[0][3], &fl[0][7]);
+          resist_flux(f[6], f[4], ez, ex, ss, sy, sz, 1, fc, &fl[1][5], &fl[1][6], &fl[1][7]);
+          fy[0 * nd + ss] = fl[0][0] + fl[1][0];
+          fy[2 * nd + ss] = fl[0][1] + fl[1][1];
+          fy[3 * nd + ss] = fl[0][2] + fl[1][2];
+          fy[1 * nd + ss] = fl[0][3] + fl[1][3];
+          fy[5 * nd + ss] = 0;
+          fy[6 * nd + ss] = fl[0][5] + fl[1][5];
+          fy[4 * nd + ss] = fl[0][6] + fl[1][6];
+          fy[7 * nd + ss] = fl[0][7] + fl[1][7];
+          rnu = 0.5 * (f[0][ss - sz] * nu[ss - sz] + f[0][ss] * nu[ss]);
+          visc_flux(vz, vx, vy, ss, rnu, idz, idx, idy, sz, 1, sy, fc, df, &fl[0][1], &fl[0][2], &fl[0][3], &fl[0][7]);
+          resist_flux(f[4], f[5], ex, ey, ss, sz, 1, sy, fc, &fl[1][5], &fl[1][6], &fl[1][7]);
+          fz[0 * nd + ss] = fl[0][0] + fl[1][0];
+          fz[3 * nd + ss] = fl[0][1] + fl[1][1];
+          fz[1 * nd + ss] = fl[0][2] + fl[1][2];
+          fz[2 * nd + ss] = fl[0][3] + fl[1][3];
+          fz[6 * nd + ss] = 0;
+          fz[4 * nd + ss] = fl[0][5] + fl[1][5];
+          fz[5 * nd + ss] = fl[0][6] + fl[1][6];
+          fz[7 * nd + ss] = fl[0][7] + fl[1][7];
+        }
+    int cen3[5] = {0, 1, 2, 3, 7};
+#pragma omp parallel for collapse(2) schedule(static) private(i, ss)
+    for (k = GH; k < nz - GH; k++)
+      for (j = GH; j < ny - GH; j++)
+        for (i = GH; i < nx - GH; i++) {
+          ss = IDX(e, i, j, k);
+          for (int c = 0; c < 5; c++) {
+            int m = cen3[c];
+            double du0 = d4(fx + (long)m * nd, ss, 1, df);
+            double du1 = d4(fy + (long)m * nd, ss, sy, df);
+            double du2 = d4(fz + (long)m * nd, ss, sz, df);
+            rk_combine(&f[m][ss], ut[(long)m * nd + ss], (-dtdx * du0 - dtdy * du1 - dtdz * du2), rkf[0], rkf[1]);
+          }
+        }
+#pragma omp parallel for collapse(2) schedule(static) private(i, ss)
+    for (k = GH; k < nz - GH + 1; k++)
+      for (j = GH; j < ny - GH + 1; j++)
+        for (i = GH; i < nx - GH + 1; i++) {
+          ss = IDX(e, i, j, k);
+          int in_k = k < nz - GH, in_j = j < ny - GH, in_i = i < nx - GH;
+          if (in_k && in_j) { /* mhd_updt3d_ctb(&bx[ss], .., &ey, &ez, dtdy, dtdz, .., nx, nxy) */
+            double du0 = +d4(ez, ss, sy, df);
+            double du1 = -d4(ey, ss, sz, df);
+            rk_combine(&f[4][ss], ut[4 * nd + ss], -dtdy * du0 - dtdz * du1, rkf[0], rkf[1]);
+          }
+          if (in_k && in_i) { /* (&by[ss], .., &ez, &ex, dtdz, dtdx, .., nxy, 1) */
+            double du0 = +d4(ex, ss, sz, df);
+            double du1 = -d4(ez, ss, 1, df);
+            rk_combine(&f[5][ss], ut[5 * nd + ss], -dtdz * du0 - dtdx * du1, rkf[0], rkf[1]);
+          }
+          if (in_j && in_i) { /* (&bz[ss], .., &ex, &ey, dtdx, dtdy, .., 1, nx) */
+            double du0 = +d4(ey, ss, 1, df);
+            double du1 = -d4(ex, ss, sy, df);
+            rk_combine(&f[6][ss], ut[6 * nd + ss], -dtdx * du0 - dtdy * du1, rkf[0], rkf[1]);
+          }
+        }
+    qo_bound(g, u);
+  }
+  free(ut); free(fx); free(fy); free(fz); free(ex); free(ey); free(ez);
+  free(vx); free(vy); free(vz); free(nu); free(eta);
+  return 0;
+}
+
 int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0)
 {
-  if (g->dim != 2) return -1;
+  if (g->dim < 2) return -1;
   double dx = g->dx, dy = g->dy;
-  double dr = qmin(dx, dy);
+  double dr = g->dim == 3 ? qmin(qmin(dx, dy), g->dz) : qmin(dx, dy);
   double dcmax = qmax(2 * nu0, eta0);
   if (dcmax < 0.0) dcmax = 0.0;
   if (dcmax > 1e-15) {

@@ -1,20 +1,43 @@
 /*
  * Oracle harness for the reference's 3D stepping code, run on one rank
- * (3D/MPI/KHI/mhd3d_solve.cpp:3-729, mhd3d_class.cpp:3-76, mpi/common_mpi.c)
- * against the single-rank MPI stand-in in oracle/mpi_stub/mpi.h.
- * Loop semantics follow MHD3D::exec_ (3D/MPI/KHI/mhd3d_class.cpp:48-76)
- * without its backup/output side effects.  Test infrastructure only.
+ * (3D/MPI/MRX/mhd3d_solve.cpp:3-729, mhd3d_class.cpp:3-76 -- identical up to
+ * whitespace to the 3D/MPI/KHI copies -- plus dmhd3d_class.cpp / dmhd3d_solve.cpp
+ * for the visco-resistive form, and mpi/common_mpi.c) against the single-rank MPI
+ * stand-in in oracle/mpi_stub/mpi.h.  Loop semantics follow MHD3D::exec_
+ * (3D/MPI/KHI/mhd3d_class.cpp:48-76) and DMHD3D::exec_ (3D/MPI/MRX/dmhd3d_class.cpp:3-40)
+ * without their backup/output side effects.  Test infrastructure only.
  */
 #include <omp.h>
-#include "mhd3d_class.hpp"
+#include "dmhd3d_class.hpp"
 #include "qas_ref_io.h"
 
 int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
 double qh_dtrec = 1.0, qh_cfl = 0.4;
 
-class RefHarness3D : public MHD3D {
+static double g_nu0 = 0.0, g_eta0 = 0.0;
+
+/* Uniform visco-resistive coefficients; same reduction as the reference's
+ * localized-profile version (3D/MPI/MRX/dmhd3d_init_.cpp:98-127; one rank). */
+double DMHD3D::setdc()
+{
+  double dcmax = 0.0, dtmp;
+  for (int k = 0; k < nz; k++) {
+    for (int j = 0; j < ny; j++) {
+      for (int i = 0; i < nx; i++) {
+        int ss = nx * (ny * k + j) + i;
+        nu[ss] = g_nu0;
+        eta[ss] = g_eta0;
+        dtmp = max(2 * nu[ss], eta[ss]);
+        if (dtmp > dcmax) dcmax = dtmp;
+      }
+    }
+  }
+  return dcmax;
+}
+
+class RefHarness3D : public DMHD3D {
  public:
-  RefHarness3D(int *argc, char ***argv) : MHD3D(argc, argv, 1) {}
+  RefHarness3D(int *argc, char ***argv) : DMHD3D(argc, argv, 1) {}
   void setup(const RefCaseHeader &h, const double *data)
   {
     setgam(h.gam);
@@ -30,12 +53,24 @@ class RefHarness3D : public MHD3D {
     for (int m = 0; m < nm; m++) { dnxs[m] = h.dnx[m]; dnys[m] = h.dny[m]; dnzs[m] = h.dnz[m]; }
     for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nd, sizeof(double) * nd);
   }
-  void one_step(int flg, std::vector<double> *dts)
+  void dissipate()
+  {
+    double dcmax = setdc();
+    if (dcmax > 1e-15) {
+      int nc, ncmax = 1 + (int)(2 * (dcmax * dt) / (dr * dr));
+      for (nc = 0; nc < ncmax; nc++) {
+        bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
+        dsptv(dt / ncmax);
+      }
+    }
+  }
+  void one_step(int flg, bool resist, std::vector<double> *dts)
   {
     tim += dt;
     dts->push_back(dt);
     bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
     ideal(dt);
+    if (resist) dissipate();
     setdt(flg * (n % 2 == 0));
   }
   int run(const RefCaseHeader &h, std::vector<double> *dts, double *elapsed)
@@ -48,19 +83,26 @@ class RefHarness3D : public MHD3D {
       bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
       ideal(dt);
       steps = 1;
-    } else if (h.mode == REF_MODE_RUN) {
+    } else if (h.mode == REF_MODE_DSTEP) {
+      dt = h.dt;
+      dts->push_back(dt);
+      setdc();
+      bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
+      dsptv(dt);
+      steps = 1;
+    } else if (h.mode == REF_MODE_RUN || h.mode == REF_MODE_DRUN) {
       setdt(1);
       for (int s = 0; s < h.nsteps; s++) {
         double ts = omp_get_wtime();
         n++;
-        one_step(h.flg, dts);
+        one_step(h.flg, h.mode == REF_MODE_DRUN, dts);
         step_times.push_back(omp_get_wtime() - ts);
         steps++;
       }
     } else if (h.mode == REF_MODE_EXEC) {
       setdt(1);
       while (n++ < nmax && tim < tmax) {
-        one_step(h.flg, dts);
+        one_step(h.flg, false, dts);
         steps++;
       }
     } else {
@@ -105,6 +147,7 @@ int main(int argc, char **argv)
   qh_rmn = h.rmn; qh_odr = h.odr; qh_rk = h.rk;
   qh_cfl = h.cfl; qh_dtrec = h.dtrec; qh_nout = h.nout;
   if (h.nthreads > 0) omp_set_num_threads(h.nthreads);
+  g_nu0 = h.nu0; g_eta0 = h.eta0;
 
   RefHarness3D *sim = new RefHarness3D(&argc, &argv);
   sim->setup(h, data.data());

@@ -24,8 +24,8 @@ enum RefMode {
   REF_MODE_STEP = 0,   /* bound(val); ideal(dt) once, with the given dt            */
   REF_MODE_RUN  = 1,   /* setdt(1); nsteps x { tim+=dt; bound; ideal; setdt(flg) } */
   REF_MODE_EXEC = 2,   /* exec_(flg) loop termination: n<nmax && tim<tmax          */
-  REF_MODE_DRUN = 3,   /* RUN with the dissipative sub-cycle after ideal (2D only) */
-  REF_MODE_DSTEP = 4,  /* bound; dsptv(dt) once (2D only)                          */
+  REF_MODE_DRUN = 3,   /* RUN with the dissipative sub-cycle after ideal (2D, 3D)  */
+  REF_MODE_DSTEP = 4,  /* bound; dsptv(dt) once (2D, 3D)                           */
   REF_MODE_IO = 5,     /* dout_ + bkup_save of the state into argv[3] (n = nsteps,
                           cnt = flg, tim = dt, dt = cfl, trec = dtrec)             */
   REF_MODE_IOLOAD = 6  /* bkup_load from argv[3]; the loaded counters go to

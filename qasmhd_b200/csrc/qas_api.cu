@@ -372,6 +372,7 @@ long long dsptv_odr(qas_ctx *c, int nc, double nu0, double eta0)
 {
   const Geo &g = c->geo;
   const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
+  const double idz = g.dim == 3 ? 1.0 / c->grid.dz : 0.0;
   long long nk = 0;
   QL(c, KID_DBOUND, k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
   QL(c, KID_DCOPY, k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, nc));
@@ -380,8 +381,9 @@ long long dsptv_odr(qas_ctx *c, int nc, double nu0, double eta0)
     double c0, c1;
     rk_factors(c->scheme.rk, rk, c0, c1);
     QL(c, KID_DVEL, k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
-    QL(c, KID_ERES, k_eres<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, eta0, idx, idy));
-    QL(c, KID_DFLUX, k_dflux<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, nu0, idx, idy));
+    QL(c, KID_ERES, k_eres<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, eta0, idx, idy, idz));
+    QL(c, KID_DFLUX,
+       k_dflux<ODR><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, nu0, idx, idy, idz));
     QL(c, KID_DUPDATE, k_dupdate<ODR><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc, c0, c1));
     QL(c, KID_DBOUND, k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, nc));
     nk += 5;
@@ -399,14 +401,16 @@ long long launch_dsptv(qas_ctx *c, int nc, double nu0, double eta0)
   }
 }
 
-// setdc + sub-cycled dsptv after ideal (dmhd2d_class.cpp:19-26), device-guarded
+// setdc + sub-cycled dsptv after ideal (dmhd2d_class.cpp:19-26, dmhd3d_class.cpp:20-28),
+// device-guarded
 long long launch_dissipate(qas_ctx *c, double nu0, double eta0)
 {
   const double dcmax0 = (2 * nu0 >= eta0) ? 2 * nu0 : eta0;
   const double dcmax = dcmax0 > 0.0 ? dcmax0 : 0.0;
   if (!(dcmax > 1e-15)) return 0;
-  QL(c, KID_DSUB, k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx, 1.0 / c->grid.dy,
-                                       NSUB_CAP));
+  const double idz = c->grid.dim == 3 ? 1.0 / c->grid.dz : 0.0;
+  QL(c, KID_DSUB, k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx,
+                                                       1.0 / c->grid.dy, NSUB_CAP, idz));
   long long nk = 1;
   for (int nc = 0; nc < NSUB_CAP; nc++) nk += launch_dsptv(c, nc, nu0, eta0);
   return nk;
@@ -427,7 +431,7 @@ long long launch_exec_step(qas_ctx *c, const qas_run_opts &o, int n_after)
   QL(c, KID_BEGIN, k_begin_step<<<1, 1, 0, c->stream>>>(c->view, o.stop_rule == 2 ? 0 : 1));
   QL(c, KID_BOUND, k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view));
   nk += 2 + launch_ideal(c);
-  if (c->grid.dim == 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
+  if (c->grid.dim >= 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
   if (o.flg && (n_after % 2 == 0)) nk += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
   return nk;
 }
@@ -733,7 +737,7 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
   qas_run_opts o = *opts;
   if (o.stop_rule < 0 || o.stop_rule > 2) return QAS_ERR_INVALID;
   if (o.stop_rule == 0 && o.max_steps <= 0) return QAS_ERR_INVALID;
-  if ((o.nu0 > 0.0 || o.eta0 > 0.0) && c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  if ((o.nu0 > 0.0 || o.eta0 > 0.0) && c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
   qas_status s;
   if (!c->run_initialised) {
     // setdt(1) of main(): dt and nmax from the initial state
@@ -827,13 +831,14 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
 qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
-  if (c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
-  k_dsub_fixed<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dt, 1.0 / c->grid.dx, 1.0 / c->grid.dy);
-  // dsptv itself does not fill the ghosts first; launch_dsptv starts with a fill, so
-  // run the body without it: copy, stages
   const Geo &g = c->geo;
   const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
+  const double idz = g.dim == 3 ? 1.0 / c->grid.dz : 0.0;
+  k_dsub_fixed<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dt, idx, idy, idz);
+  // dsptv itself does not fill the ghosts first; launch_dsptv starts with a fill, so
+  // run the body without it: copy, stages
   k_dcopy<<<(unsigned)((g.nd + 255) / 256), 256, 0, c->stream>>>(c->view, c->d_dctl, 0);
   long long nk = 2;
   for (int rk = 0; rk < c->scheme.rk; rk++) {
@@ -843,8 +848,8 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 #define QAS_DST(O)                                                                                        \
   case O:                                                                                                 \
     k_dvel<<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                  \
-    k_eres<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, eta0, idx, idy);               \
-    k_dflux<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, nu0, idx, idy);               \
+    k_eres<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, eta0, idx, idy, idz);          \
+    k_dflux<O><<<cells_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, nu0, idx, idy, idz);          \
     k_dupdate<O><<<update_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0, c0, c1);                   \
     k_dbound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view, c->d_dctl, 0);                                \
     break;
@@ -864,7 +869,7 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
-  if (c->grid.dim != 2) return QAS_ERR_UNSUPPORTED;
+  if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
   c->launches += 1 + launch_dissipate(c, nu0, eta0);

@@ -1,6 +1,8 @@
-// qas_dissip.cuh -- visco-resistive update of the 2D driver on sm_100a:
-// DMHD2D::dsptv (2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151) with uniform nu, eta,
-// sub-cycled as in DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26).
+// qas_dissip.cuh -- visco-resistive update of the 2D and 3D drivers on sm_100a:
+// DMHD2D::dsptv (2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151) and DMHD3D::dsptv
+// (3D/MPI/MRX/dmhd3d_solve.cpp:3-179) with uniform nu, eta, sub-cycled as in
+// DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26) and DMHD3D::exec_
+// (3D/MPI/MRX/dmhd3d_class.cpp:20-28).
 #pragma once
 
 #include "qas_kernels.cuh"
@@ -12,11 +14,12 @@ struct DCtl {
   int ncmax;
   int pad;
   double sdt;      // dt/ncmax
-  double sdtd[2];  // sdt*idx, sdt*idy
+  double sdtd[3];  // sdt*idx, sdt*idy, sdt*idz (dtdx = dt*idx as in dsptv)
 };
 
 // setdc + ncmax = 1 + (int)(2*(dcmax*dt)/(dr*dr))
-__global__ void k_dsub_setup(View v, DCtl *dc, double dcmax, double dr, double idx, double idy, int cap)
+__global__ void k_dsub_setup(View v, DCtl *dc, double dcmax, double dr, double idx, double idy, int cap,
+                             double idz = 0.0)
 {
   if (v.ctl->done) return;
   const double dt = v.ctl->dt;
@@ -30,15 +33,17 @@ __global__ void k_dsub_setup(View v, DCtl *dc, double dcmax, double dr, double i
   dc->sdt = ncmax > 0 ? dt / ncmax : 0.0;
   dc->sdtd[0] = dc->sdt * idx;
   dc->sdtd[1] = dc->sdt * idy;
+  dc->sdtd[2] = dc->sdt * idz;
 }
 
 // host-supplied dt for one dsptv(dt) call
-__global__ void k_dsub_fixed(View v, DCtl *dc, double dt, double idx, double idy)
+__global__ void k_dsub_fixed(View v, DCtl *dc, double dt, double idx, double idy, double idz)
 {
   dc->ncmax = 1;
   dc->sdt = dt;
   dc->sdtd[0] = dt * idx;
   dc->sdtd[1] = dt * idy;
+  dc->sdtd[2] = dt * idz;
 }
 
 #define QAS_DSUB_GUARD()                        \
@@ -56,21 +61,31 @@ __global__ void k_dvel(View v, const DCtl *dc, int nc)
   v.vz[c] = v.u[3][c] * iro;
 }
 
-// eta*J on the CT edges, mhd_ct_eres (common/mhd_func.c:78-106) with zoffset=0, idz=0
+// eta*J on the CT edges, mhd_ct_eres (common/mhd_func.c:78-106): in 2D with zoffset = 0 and
+// idz = 0 (dmhd2d_solve.cpp:46-54), in 3D with the real z stencils (dmhd3d_solve.cpp:48-57)
 template <int ODR>
-__global__ void k_eres(View v, const DCtl *dc, int nc, double eta0, double idx, double idy)
+__global__ void k_eres(View v, const DCtl *dc, int nc, double eta0, double idx, double idy, double idz3 = 0.0)
 {
   QAS_DSUB_GUARD();
   QAS_CELL_INDEX();
   const Geo &g = v.g;
   if (i < 2 || i >= g.nx - 1 || j < 2 || j >= g.ny - 1) return;
+  if (g.dim == 3 && (k < 2 || k >= g.nz - 1)) return;
   const long long c = cidx(g, i, j, k);
   const long long sy = g.s[1];
   const double *bx = v.u[4], *by = v.u[5], *bz = v.u[6];
-  const double idz = 0.0;
-  // derivatives along the absent z axis see four equal values
-  const double dbxz = dfc<ODR>(bx[c], bx[c], bx[c], bx[c]);
-  const double dbyz = dfc<ODR>(by[c], by[c], by[c], by[c]);
+  double dbxz, dbyz, idz;
+  if (g.dim == 3) {
+    const long long sz = g.s[2];
+    idz = idz3;
+    dbxz = dfc<ODR>(bx[c - 2 * sz], bx[c - sz], bx[c], bx[c + sz]);
+    dbyz = dfc<ODR>(by[c - 2 * sz], by[c - sz], by[c], by[c + sz]);
+  } else {
+    // derivatives along the absent z axis see four equal values
+    idz = 0.0;
+    dbxz = dfc<ODR>(bx[c], bx[c], bx[c], bx[c]);
+    dbyz = dfc<ODR>(by[c], by[c], by[c], by[c]);
+  }
   const double jx = dfc<ODR>(bz[c - 2 * sy], bz[c - sy], bz[c], bz[c + sy]) * idy - dbyz * idz;
   const double jy = dbxz * idz - dfc<ODR>(bz[c - 2], bz[c - 1], bz[c], bz[c + 1]) * idx;
   const double jz = dfc<ODR>(by[c - 2], by[c - 1], by[c], by[c + 1]) * idx -
@@ -145,20 +160,24 @@ __device__ __forceinline__ void resist_flux(const double *by, const double *bz, 
 }
 
 template <int ODR>
-__global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, double idy)
+__global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, double idy, double idz3 = 0.0)
 {
   QAS_DSUB_GUARD();
   QAS_CELL_INDEX();
   const Geo &g = v.g;
   if (i < 2 || i >= g.nx - 1 || j < 2 || j >= g.ny - 1) return;
+  const bool d3 = g.dim == 3;
+  if (d3 && (k < 2 || k >= g.nz - 1)) return;
   const long long c = cidx(g, i, j, k);
   const long long sy = g.s[1];
+  const long long sz = d3 ? g.s[2] : 0;  // the absent axis has offset 0 and idz 0 in 2D
+  const double idz = d3 ? idz3 : 0.0;
   const double *ro = v.u[0];
   double fmx, fmy, fmz, fenv, fby, fbz, fenr;
-  // x face (dmhd2d_solve.cpp:70-82)
+  // x face (dmhd2d_solve.cpp:70-82, dmhd3d_solve.cpp:72-84)
   double rnu = 0.5 * (ro[c - 1] * nu0 + ro[c] * nu0);
-  visc_flux<ODR>(v.vx, v.vy, v.vz, c, rnu, idx, idy, 0.0, 1, sy, 0, fmx, fmy, fmz, fenv);
-  resist_flux<ODR>(v.u[5], v.u[6], v.ey, v.ez, c, 1, sy, 0, fby, fbz, fenr);
+  visc_flux<ODR>(v.vx, v.vy, v.vz, c, rnu, idx, idy, idz, 1, sy, sz, fmx, fmy, fmz, fenv);
+  resist_flux<ODR>(v.u[5], v.u[6], v.ey, v.ez, c, 1, sy, sz, fby, fbz, fenr);
   v.f[0][0][c] = 0.0 + 0.0;
   v.f[0][1][c] = fmx + 0.0;
   v.f[0][2][c] = fmy + 0.0;
@@ -166,10 +185,10 @@ __global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, 
   v.f[0][5][c] = 0.0 + fby;
   v.f[0][6][c] = 0.0 + fbz;
   v.f[0][7][c] = fenv + fenr;
-  // y face (dmhd2d_solve.cpp:83-94)
+  // y face (dmhd2d_solve.cpp:83-94, dmhd3d_solve.cpp:86-97)
   rnu = 0.5 * (ro[c - sy] * nu0 + ro[c] * nu0);
-  visc_flux<ODR>(v.vy, v.vz, v.vx, c, rnu, idy, 0.0, idx, sy, 0, 1, fmx, fmy, fmz, fenv);
-  resist_flux<ODR>(v.u[6], v.u[4], v.ez, v.ex, c, sy, 0, 1, fby, fbz, fenr);
+  visc_flux<ODR>(v.vy, v.vz, v.vx, c, rnu, idy, idz, idx, sy, sz, 1, fmx, fmy, fmz, fenv);
+  resist_flux<ODR>(v.u[6], v.u[4], v.ez, v.ex, c, sy, sz, 1, fby, fbz, fenr);
   v.f[1][0][c] = 0.0 + 0.0;
   v.f[1][2][c] = fmx + 0.0;
   v.f[1][3][c] = fmy + 0.0;
@@ -177,16 +196,25 @@ __global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, 
   v.f[1][6][c] = 0.0 + fby;
   v.f[1][4][c] = 0.0 + fbz;
   v.f[1][7][c] = fenv + fenr;
+  if (d3) {  // z face (dmhd3d_solve.cpp:99-110)
+    rnu = 0.5 * (ro[c - sz] * nu0 + ro[c] * nu0);
+    visc_flux<ODR>(v.vz, v.vx, v.vy, c, rnu, idz, idx, idy, sz, 1, sy, fmx, fmy, fmz, fenv);
+    resist_flux<ODR>(v.u[4], v.u[5], v.ex, v.ey, c, sz, 1, sy, fby, fbz, fenr);
+    v.f[2][0][c] = 0.0 + 0.0;
+    v.f[2][3][c] = fmx + 0.0;
+    v.f[2][1][c] = fmy + 0.0;
+    v.f[2][2][c] = fmz + 0.0;
+    v.f[2][4][c] = 0.0 + fby;
+    v.f[2][5][c] = 0.0 + fbz;
+    v.f[2][7][c] = fenv + fenr;
+  }
 }
 
+// RK update of the 2D dsptv (dmhd2d_solve.cpp:107-146)
 template <int ODR>
-__global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
+__device__ __forceinline__ void dupdate2(const View &v, const DCtl *dc, int i, int j, double c0, double c1)
 {
-  QAS_DSUB_GUARD();
   const Geo &g = v.g;
-  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = GH + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i > g.nx - GH || j > g.ny - GH || blockIdx.z * blockDim.z + threadIdx.z > 0) return;
   const long long c = cidx(g, i, j, 0);
   const long long sy = g.s[1];
   const double dtdx = dc->sdtd[0], dtdy = dc->sdtd[1];
@@ -217,6 +245,71 @@ __global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
   }
   if (cj) v.u[4][c] = nbx;
   if (ci) v.u[5][c] = nby;
+}
+
+// RK update of the 3D dsptv (dmhd3d_solve.cpp:114-167): mhd_updt3d on ro,mx,my,mz,en over the
+// interior, mhd_updt3d_ctb on bx (one extra face along x), by (along y) and bz (along z)
+template <int ODR>
+__device__ __forceinline__ void dupdate3(const View &v, const DCtl *dc, int i, int j, int k, double c0, double c1)
+{
+  const Geo &g = v.g;
+  const long long c = cidx(g, i, j, k);
+  const long long sy = g.s[1], sz = g.s[2];
+  const double dtdx = dc->sdtd[0], dtdy = dc->sdtd[1], dtdz = dc->sdtd[2];
+  const bool ci = i < g.nx - GH, cj = j < g.ny - GH, ck = k < g.nz - GH;
+  const int cen[5] = {0, 1, 2, 3, 7};
+  double nv[5], nb[3] = {0.0, 0.0, 0.0};
+  if (ci && cj && ck) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      const int m = cen[q];
+      const double du0 = d4<ODR>(v.f[0][m], c, 1);
+      const double du1 = d4<ODR>(v.f[1][m], c, sy);
+      const double du2 = d4<ODR>(v.f[2][m], c, sz);
+      nv[q] = rk_combine(v.u[m][c], v.u0[m][c], (-dtdx * du0 - dtdy * du1 - dtdz * du2), c0, c1);
+    }
+  }
+  if (cj && ck) {
+    const double du0 = +d4<ODR>(v.ez, c, sy);
+    const double du1 = -d4<ODR>(v.ey, c, sz);
+    nb[0] = rk_combine(v.u[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
+  }
+  if (ci && ck) {
+    const double du0 = +d4<ODR>(v.ex, c, sz);
+    const double du1 = -d4<ODR>(v.ez, c, 1);
+    nb[1] = rk_combine(v.u[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
+  }
+  if (ci && cj) {
+    const double du0 = +d4<ODR>(v.ey, c, 1);
+    const double du1 = -d4<ODR>(v.ex, c, sy);
+    nb[2] = rk_combine(v.u[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
+  }
+  if (ci && cj && ck) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) v.u[cen[q]][c] = nv[q];
+  }
+  if (cj && ck) v.u[4][c] = nb[0];
+  if (ci && ck) v.u[5][c] = nb[1];
+  if (ci && cj) v.u[6][c] = nb[2];
+}
+
+template <int ODR>
+__global__ void k_dupdate(View v, const DCtl *dc, int nc, double c0, double c1)
+{
+  QAS_DSUB_GUARD();
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = GH + blockIdx.y * blockDim.y + threadIdx.y;
+  const int kt = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > g.nx - GH || j > g.ny - GH) return;
+  if (g.dim == 3) {
+    const int k = GH + kt;
+    if (k > g.nz - GH) return;
+    dupdate3<ODR>(v, dc, i, j, k, c0, c1);
+  } else {
+    if (kt > 0) return;
+    dupdate2<ODR>(v, dc, i, j, c0, c1);
+  }
 }
 
 __global__ void k_dbound(View v, const DCtl *dc, int nc)

@@ -83,6 +83,13 @@ def _kh2_eta():
     return p
 
 
+def _wave3_eta(ctw, nu0, eta0, rmn=P.RMN_HLLD):
+    """3D visco-resistive case (DMHD3D::dsptv); eta0=0.3 gives two sub-cycles per step."""
+    p = P.smooth_wave(3, 8, ctw=ctw, rmn=rmn)
+    p.nu0, p.eta0 = nu0, eta0
+    return p
+
+
 def _wave_bc(dim, seed):
     rng = np.random.default_rng(seed)
 
@@ -106,6 +113,8 @@ STEP_CASES = [
     ("ot2d_exec", lambda: P.orszag_tang(16, tmax=0.05), R.MODE_EXEC, 0),
     ("kh2d_mlau", lambda: P.kelvin_helmholtz(2, 16, mach=0.3, rmn=P.RMN_MLAU), R.MODE_RUN, 3),
     ("kh2d_roe_eta", _kh2_eta, R.MODE_DRUN, 3),
+    ("wave3d_eta_ctw1", lambda: _wave3_eta(1, 0.02, 0.05), R.MODE_DRUN, 2),
+    ("wave3d_eta_ctw0_sub2", lambda: _wave3_eta(0, 0.05, 0.3, rmn=P.RMN_ROE), R.MODE_DRUN, 2),
     *[(f"kh3d_rmn{r}", (lambda r=r: P.kelvin_helmholtz(3, 6, mach=0.3, rmn=r)), R.MODE_RUN, 2) for r in range(4)],
     *[(f"wave{d}d_bc{s}", (lambda d=d, s=s: _wave_bc(d, s)), R.MODE_RUN, 2) for d in (1, 2, 3) for s in (1, 2)],
 ]

@@ -65,3 +65,17 @@ def test_live_reference_dissipative(restatement):
     a = R.run_reference(p, R.MODE_DSTEP, dt=2e-3, nthreads=2)
     b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
     assert_bitwise(b["state"], a["state"], "dstep")
+
+
+@needs_ref
+@pytest.mark.parametrize("ctw", [0, 1])
+def test_live_reference_dissipative_3d(restatement, ctw):
+    """DMHD3D::dsptv (3D/MPI/MRX/dmhd3d_solve.cpp) and the sub-cycled exec_ loop around it."""
+    p = P.smooth_wave(3, 7, ctw=ctw, rmn=P.RMN_MLAU, seed=3)
+    p.nu0, p.eta0 = 0.04, 0.25
+    a = R.run_reference(p, R.MODE_DSTEP, dt=2e-3, nthreads=2)
+    b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
+    assert_bitwise(b["state"], a["state"], "dstep3d")
+    a = R.run_reference(p, R.MODE_DRUN, nsteps=2, nthreads=2)
+    b = restatement.run(p, 2, mode=R.MODE_DRUN)
+    assert_bitwise(b["state"], a["state"], "drun3d")

@@ -69,6 +69,26 @@ def test_single_dsptv(restatement):
     assert_bitwise(b["state"], a["state"], "dsptv")
 
 
+@pytest.mark.parametrize("odr", [2, 4])
+def test_single_dsptv_3d(restatement, odr):
+    p = P.smooth_wave(3, 20, odr=odr, seed=5)
+    p.nu0, p.eta0 = 3e-3, 4e-3
+    a = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
+    b = run_gpu(p, R.MODE_DSTEP, dt=2e-3)
+    assert_bitwise(b["state"], a["state"], f"dsptv3d odr{odr}")
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_dissipative_run_3d(restatement, use_graph):
+    """exec_ of DMHD3D: ideal step, then the sub-cycled dsptv (two sub-cycles here)."""
+    p = P.kelvin_helmholtz(3, 16, mach=0.3, rmn=P.RMN_HLLD)
+    p.nu0, p.eta0 = 0.01, 0.1
+    a = restatement.run(p, 4, mode=R.MODE_DRUN)
+    assert np.isfinite(a["state"]).all()
+    b = run_gpu(p, R.MODE_DRUN, 4, use_graph=use_graph)
+    assert_bitwise(b["state"], a["state"], "drun3d")
+
+
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_graph_and_eager_agree(restatement, use_graph):
     p = P.orszag_tang(48)
