@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "bw1d_1024"], default="ot2d_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lr-staging", type=int, choices=[0, 1], default=None,
+                    help="reconstruction stencils: 1 = TMA-staged in shared memory, 0 = global loads "
+                         "(default: the library's default for the grid)")
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
@@ -59,7 +62,23 @@ def parse():
                     help="print only the adjoint comparison over --steps steps (profiling aid)")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="print only the batched-ensemble comparison over --steps steps (profiling aid)")
+    ap.add_argument("--lr-forms-case", action="store_true",
+                    help="profiling aid: one eager exec_ step of Orszag-Tang 512^2 with the global-load "
+                         "reconstruction, then one with the TMA-staged reconstruction; prints nothing timed")
     return ap.parse_args()
+
+
+def lr_forms_case():
+    from qasmhd_b200 import lib as L
+    from qasmhd_b200 import problems as P
+    p = P.orszag_tang(512)
+    for st in (0, 1):
+        with L.Context.from_problem(p) as ctx:
+            ctx.set_option(L.QAS_OPT_LR_STAGING, st)
+            ctx.upload(p.state)
+            ctx.run(max_steps=1, flg=1, stop_rule=0, cfl=p.cfl, use_graph=False)
+            ctx.download(p.state.shape)
+    print(json.dumps({"lr_forms_case": "ok"}))
 
 
 def make_problem(name):
@@ -278,6 +297,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.lr_forms_case:
+        if rank == 0:
+            lr_forms_case()
+        return
     if args.adjoint_only or args.ensemble_only:
         if rank == 0:
             out = {}
@@ -294,6 +317,8 @@ def main():
     prob, cfg = make_problem(args.workload)
     cells = prob.interior_cells
     ctx = L.Context.from_problem(prob, device=local)
+    if args.lr_staging is not None:
+        ctx.set_option(L.QAS_OPT_LR_STAGING, args.lr_staging)
     ctx.upload(prob.state)
     ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
 

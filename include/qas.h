@@ -184,8 +184,13 @@ qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, q
 /* Tuning options (defaults are the measured best on B200).
  *   QAS_OPT_FUSED_SWEEP: 0 = reconstruction and Riemann flux of each direction in two
  *   kernels with the face states in HBM (default); 1 = one fused sweep kernel.
- * Both forms give bit-identical results. */
+ *   QAS_OPT_LR_STAGING: 1 = the reconstruction stages its stencils in shared memory with
+ *   TMA tensor copies (available for 2D/3D, 4th-order interpolation, even padded x extent;
+ *   QAS_ERR_UNSUPPORTED otherwise); 0 = it reads them from global memory (default: measured
+ *   faster on B200, where this kernel is bound by FP64 dependency latency, not by loads).
+ * All forms give bit-identical results. */
 #define QAS_OPT_FUSED_SWEEP 1
+#define QAS_OPT_LR_STAGING 2
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

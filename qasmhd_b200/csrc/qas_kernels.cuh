@@ -202,16 +202,66 @@ __global__ void k_dv(View v)
 #ifndef QAS_LR_MINB
 #define QAS_LR_MINB 5
 #endif
-#ifndef QAS_LR_GROUPED
-#define QAS_LR_GROUPED 1
-#endif
 
-// stencil accessor of k_lr's grouped form: primitive v at point m (0..4) of cell c
+// stencil accessor of k_lr: field f of (ro, vn, vb, vc, cb, cc, pr) along axis A at point m
+// (0..4) of cell c; the field pointers are read from the kernel's View parameter at each use,
+// so no pointer stays live in registers
+template <int A>
 struct LrStencil {
-  const double *p[7];
+  const View &v;
   long long c, s;
-  __device__ __forceinline__ double operator()(int v, int m) const { return __ldg(p[v] + c + (m - 2) * s); }
+  __device__ __forceinline__ const double *field(int f) const
+  {
+    constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+    switch (f) {
+      case 0: return v.u[0];
+      case 1: return A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
+      case 2: return B == 0 ? v.vx : (B == 1 ? v.vy : v.vz);
+      case 3: return C == 0 ? v.vx : (C == 1 ? v.vy : v.vz);
+      case 4: return B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
+      case 5: return C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
+      default: return v.pr;
+    }
+  }
+  __device__ __forceinline__ double operator()(int f, int m) const { return __ldg(field(f) + c + (m - 2) * s); }
+  // plain load, for reads issued after the face-state stores (kept in order behind them)
+  __device__ __forceinline__ double late(int f, int m) const { return field(f)[c + (m - 2) * s]; }
 };
+
+template <int ODR, int A, class ST>
+__device__ __forceinline__ void lr_cell(const View &v, long long c, long long s, const ST &st, double cnc)
+{
+  double vl[7], vr[7];
+  face_states_grouped<ODR>(st, cnc, v.gam, vl, vr);
+#pragma unroll
+  for (int m = 0; m < 7; m++) {
+    v.vl[m][c] = vl[m];
+    v.vr[m][c] = vr[m];
+  }
+  if (v.g.dim >= 2) {
+    // the induction states are read after the face states are stored (keeps their loads from
+    // being hoisted over the reconstruction, which would raise register pressure)
+    asm volatile("" ::: "memory");
+    const double *bnf = v.u[4 + A];
+    const double bfl = bnf[c + s], bfr = bnf[c];
+    // transverse component t0 = B axis (used in 3D; in 2D along x), t1 = C axis (3D; 2D along y)
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      if (v.g.dim == 2 && ((A == 0 && t == 1) || (A == 1 && t == 0))) continue;
+      double prod[5], vts[5];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        prod[m] = st.late(4 + t, m) * st.late(1, m);  // bt * vn
+        vts[m] = st.late(2 + t, m);                   // vt
+      }
+      double fl0, fr0, fl1, fr1;
+      lin_lr<ODR>(prod, fl0, fr0);
+      lin_lr<ODR>(vts, fl1, fr1);
+      v.ql[t][c] = fl0 - bfl * fl1;
+      v.qr[t][c] = fr0 - bfr * fr1;
+    }
+  }
+}
 
 template <int ODR, int A>
 __device__ __forceinline__ void lr_body(const View &v, int i, int j, int k)
@@ -222,60 +272,9 @@ __device__ __forceinline__ void lr_body(const View &v, int i, int j, int k)
   if (pos < 2 || pos >= n - 2) return;
   const long long c = cidx(g, i, j, k);
   const long long s = g.s[A];
-  constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
-  const double *vn = A == 0 ? v.vx : (A == 1 ? v.vy : v.vz);
-  const double *vb = B == 0 ? v.vx : (B == 1 ? v.vy : v.vz);
-  const double *vc = C == 0 ? v.vx : (C == 1 ? v.vy : v.vz);
   const double *cn = A == 0 ? v.cx : (A == 1 ? v.cy : v.cz);
-  const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
-  const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
-  const double *bnf = v.u[4 + A];
-  double vl[7], vr[7];
-#if QAS_LR_GROUPED
-  const LrStencil st{{v.u[0], vn, vb, vc, cb, ccp, v.pr}, c, s};
-  face_states_grouped<ODR>(st, cn[c], v.gam, vl, vr);
-#else
-  double q[7][5];
-#pragma unroll
-  for (int m = 0; m < 5; m++) {
-    const long long p = c + (m - 2) * s;
-    q[0][m] = v.u[0][p];
-    q[1][m] = vn[p];
-    q[2][m] = vb[p];
-    q[3][m] = vc[p];
-    q[4][m] = cb[p];
-    q[5][m] = ccp[p];
-    q[6][m] = v.pr[p];
-  }
-  face_states<ODR>(q, cn[c], v.gam, vl, vr);
-#endif
-#pragma unroll
-  for (int m = 0; m < 7; m++) {
-    v.vl[m][c] = vl[m];
-    v.vr[m][c] = vr[m];
-  }
-  if (g.dim >= 2) {
-    const double bfl = bnf[c + s], bfr = bnf[c];
-    // transverse component t0 = B axis (used in 3D; in 2D along x), t1 = C axis (3D; 2D along y)
-#pragma unroll
-    for (int t = 0; t < 2; t++) {
-      if (g.dim == 2 && ((A == 0 && t == 1) || (A == 1 && t == 0))) continue;
-      const double *vt = t == 0 ? vb : vc;
-      const double *bt = t == 0 ? cb : ccp;
-      double prod[5], vts[5];
-#pragma unroll
-      for (int m = 0; m < 5; m++) {
-        const long long p = c + (m - 2) * s;
-        prod[m] = bt[p] * vn[p];
-        vts[m] = vt[p];
-      }
-      double fl0, fr0, fl1, fr1;
-      lin_lr<ODR>(prod, fl0, fr0);
-      lin_lr<ODR>(vts, fl1, fr1);
-      v.ql[t][c] = fl0 - bfl * fl1;
-      v.qr[t][c] = fr0 - bfr * fr1;
-    }
-  }
+  const LrStencil<A> st{v, c, s};
+  lr_cell<ODR, A>(v, c, s, st, cn[c]);
 }
 template <int ODR, int A>
 __global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
@@ -376,7 +375,7 @@ __device__ __forceinline__ void cell_states(const View &v, long long c, double v
   const double *cn = A == 0 ? v.cx : (A == 1 ? v.cy : v.cz);
   const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
   const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
-  const LrStencil st{{v.u[0], vn, vb, vc, cb, ccp, v.pr}, c, s};
+  const LrStencil<A> st{v, c, s};
   face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
   if (g.dim >= 2) {
     const double *bnf = v.u[4 + A];

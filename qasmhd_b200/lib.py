@@ -40,6 +40,7 @@ EXPORTS = (
     "qas_bkup_load",
 )
 QAS_OPT_FUSED_SWEEP = 1
+QAS_OPT_LR_STAGING = 2
 
 
 class QasError(RuntimeError):
