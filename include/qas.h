@@ -259,6 +259,41 @@ qas_status qas_bkup_load(qas_ctx *ctx, const char *dir, int rank, int *loaded, i
                          double *dt, double *trec);
 
 /* ------------------------------------------------------------------------------------
+ * One domain split into slabs along its last axis (z in 3D, y in 2D), each slab a context on
+ * its own GPU (or several on one): the reference's rank decomposition and halo driver
+ * (mpi/common_mpi.c:198-525, mpi_sdrv3d + mpi_x/y/zbc3d; the MPI_Allreduce(MAX) of the CFL
+ * speed in MHD3D::setdt, 3D/MPI/KHI/mhd3d_class.cpp:15-46) inside one process.  Ghost planes
+ * whose source is another slab (internal boundaries, the wrap of a periodic axis) are copied
+ * from it (peer copies between GPUs) after each ghost fill, after the primitives and after
+ * the shock detector; the control block is replicated; results are bit-identical to the
+ * single-domain context.  The split axis must be periodic for all 8 fields or physical for
+ * all 8 (QAS_ERR_UNSUPPORTED otherwise), and each slab needs >= 8 planes.  Ideal MHD only
+ * (QAS_ERR_UNSUPPORTED for nu0/eta0 > 0).
+ * qas_dd_plan: the split (lo[0..nparts], global interior plane offsets) and the ghost-plane
+ * copies of a decomposition, host only (no device needed).
+ * devices: nparts CUDA device ordinals, or NULL for the current device.
+ * Blocks: 8 fields over the GLOBAL padded grid, the layout of qas_upload_block.
+ * ------------------------------------------------------------------------------------ */
+typedef struct qas_dd qas_dd;
+typedef struct {
+  int part;       /* slab whose ghost planes are written               */
+  int src_part;   /* slab that holds the source planes                 */
+  int src_plane;  /* first source plane (padded index along the axis)  */
+  int dst_plane;  /* first ghost plane                                 */
+  int nplanes;    /* always 4                                          */
+} qas_dd_copy;
+qas_status qas_dd_plan(const qas_grid *grid, const qas_bc *bc, int nparts, int *lo, qas_dd_copy *copies,
+                       int max_copies, int *ncopies);
+qas_status qas_dd_create(qas_dd **dd, const qas_grid *grid, const qas_scheme *scheme, const qas_bc *bc, int nparts,
+                         const int *devices);
+qas_status qas_dd_destroy(qas_dd *dd);
+qas_status qas_dd_upload_block(qas_dd *dd, const double *block);
+qas_status qas_dd_download_block(qas_dd *dd, double *block);
+qas_status qas_dd_run(qas_dd *dd, const qas_run_opts *opts, qas_run_info *info);
+qas_status qas_dd_parts(const qas_dd *dd, int *nparts);
+qas_status qas_dd_kernel_launches(const qas_dd *dd, long long *kernels, long long *copies);
+
+/* ------------------------------------------------------------------------------------
  * Discrete adjoint of the 2D step (no counterpart in the reference, which has no
  * derivatives): the exec_ step body -- bound(), ideal(dt) (MHD2D::ideal,
  * 2D/SERIAL/OTvortex/mhd2d_solve.cpp:3-400) and, with eta0 > 0, setdc + the sub-cycled

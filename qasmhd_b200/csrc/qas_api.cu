@@ -446,17 +446,26 @@ void launch_sweep(qas_ctx *c, int a)
   }
 }
 
+// one SSP-RK stage in three phases (a domain split into slabs exchanges ghost planes
+// between them): primitives + cell-centre B; the shock detector; sweeps, EMF, update, fill
 template <int ODR>
-long long stage_odr(qas_ctx *c, double c0, double c1)
+long long stage_prim(qas_ctx *c)
+{
+  QL(c, KID_PRIM, k_prim<ODR><<<cells_grid(c->geo, c->tile[KID_PRIM]), c->tile[KID_PRIM], 0, c->stream>>>(c->view));
+  return 1;
+}
+bool stage_has_dv(const qas_ctx *c) { return c->scheme.rmn >= 2 && c->geo.dim >= 2; }
+long long stage_dv(qas_ctx *c)
+{
+  if (!stage_has_dv(c)) return 0;
+  QL(c, KID_DV, k_dv<<<cells_grid(c->geo, c->tile[KID_DV]), c->tile[KID_DV], 0, c->stream>>>(c->view));
+  return 1;
+}
+template <int ODR>
+long long stage_rest(qas_ctx *c, double c0, double c1)
 {
   const Geo &g = c->geo;
   long long nk = 0;
-  QL(c, KID_PRIM, k_prim<ODR><<<cells_grid(g, c->tile[KID_PRIM]), c->tile[KID_PRIM], 0, c->stream>>>(c->view));
-  nk++;
-  if (c->scheme.rmn >= 2 && g.dim >= 2) {
-    QL(c, KID_DV, k_dv<<<cells_grid(g, c->tile[KID_DV]), c->tile[KID_DV], 0, c->stream>>>(c->view));
-    nk++;
-  }
   for (int a = 0; a < g.dim; a++) {
     if (c->fused) {
       switch (c->scheme.rmn) {
@@ -485,6 +494,34 @@ long long stage_odr(qas_ctx *c, double c0, double c1)
   QL(c, KID_BOUND, k_bound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view));
   nk += 2;
   return nk;
+}
+
+template <int ODR>
+long long stage_odr(qas_ctx *c, double c0, double c1)
+{
+  long long nk = stage_prim<ODR>(c);
+  nk += stage_dv(c);
+  return nk + stage_rest<ODR>(c, c0, c1);
+}
+
+// phase helpers by run-time order
+long long stage_prim_any(qas_ctx *c)
+{
+  switch (c->scheme.odr) {
+    case 1: return stage_prim<1>(c);
+    case 2: return stage_prim<2>(c);
+    case 3: return stage_prim<3>(c);
+    default: return stage_prim<4>(c);
+  }
+}
+long long stage_rest_any(qas_ctx *c, double c0, double c1)
+{
+  switch (c->scheme.odr) {
+    case 1: return stage_rest<1>(c, c0, c1);
+    case 2: return stage_rest<2>(c, c0, c1);
+    case 3: return stage_rest<3>(c, c0, c1);
+    default: return stage_rest<4>(c, c0, c1);
+  }
 }
 
 // rk_fac table of mhd2d_solve.cpp:7 for the context's R_K
@@ -1345,3 +1382,4 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 #include "qas_adjoint_api.inc"
 #include "qas_noalloc.inc"
 #include "qas_io.inc"
+#include "qas_dd.inc"

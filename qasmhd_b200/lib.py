@@ -37,7 +37,8 @@ EXPORTS = (
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
     "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
     "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
-    "qas_bkup_load",
+    "qas_bkup_load", "qas_dd_plan", "qas_dd_create", "qas_dd_destroy", "qas_dd_upload_block",
+    "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches",
 )
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
@@ -76,6 +77,11 @@ class RunOpts(ctypes.Structure):
 
 class KernelTime(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_longlong), ("total_ms", ctypes.c_double)]
+
+
+class DdCopy(ctypes.Structure):
+    _fields_ = [("part", ctypes.c_int), ("src_part", ctypes.c_int), ("src_plane", ctypes.c_int),
+                ("dst_plane", ctypes.c_int), ("nplanes", ctypes.c_int)]
 
 
 class RunInfo(ctypes.Structure):
@@ -154,6 +160,17 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                          ctypes.c_void_p, dp]
     lib.qas_bc_map.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.qas_dd_plan.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(BC), ctypes.c_int, ip, ctypes.POINTER(DdCopy),
+                                ctypes.c_int, ip]
+    lib.qas_dd_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Grid), ctypes.POINTER(Scheme),
+                                  ctypes.POINTER(BC), ctypes.c_int, ip]
+    lib.qas_dd_destroy.argtypes = [vp]
+    lib.qas_dd_upload_block.argtypes = [vp, dp]
+    lib.qas_dd_download_block.argtypes = [vp, dp]
+    lib.qas_dd_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
+    lib.qas_dd_parts.argtypes = [vp, ip]
+    lib.qas_dd_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     for name in EXPORTS:
         if name not in ("qas_status_str", "qas_abi_version", "qas_last_cuda_error"):
             getattr(lib, name).restype = ctypes.c_int
@@ -385,6 +402,77 @@ def bc_map(prob, group: int, field: int, axis: int):
     _check(lib.qas_bc_map(ctypes.byref(g), ctypes.byref(b), group, field, axis,
                           src.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(fac), n), "qas_bc_map")
     return src, fac
+
+
+def dd_plan(prob, nparts: int):
+    """Host-only: the slab split (global interior plane offsets, nparts+1 entries) and the
+    ghost-plane copies [(part, src_part, src_plane, dst_plane, nplanes)] of a decomposition
+    (qas_dd_plan)."""
+    lib = load()
+    g, _, b = _grid_scheme_bc(prob)
+    lo = (ctypes.c_int * (nparts + 1))()
+    cnt = ctypes.c_int()
+    _check(lib.qas_dd_plan(ctypes.byref(g), ctypes.byref(b), int(nparts), lo, None, 0, ctypes.byref(cnt)),
+           "qas_dd_plan")
+    cps = (DdCopy * max(cnt.value, 1))()
+    _check(lib.qas_dd_plan(ctypes.byref(g), ctypes.byref(b), int(nparts), lo, cps, cnt.value, ctypes.byref(cnt)),
+           "qas_dd_plan")
+    return list(lo), [(c.part, c.src_part, c.src_plane, c.dst_plane, c.nplanes) for c in cps[:cnt.value]]
+
+
+class Decomposition:
+    """One domain split into slabs along its last axis, each slab a context on its own device
+    (or several on one): qas_dd_* (the reference's MPI rank decomposition in one process)."""
+
+    def __init__(self, prob, nparts: int, devices: Optional[Sequence[int]] = None):
+        self.lib = load()
+        g, sc, b = _grid_scheme_bc(prob)
+        devs = None
+        if devices is not None:
+            devs = (ctypes.c_int * nparts)(*[int(d) for d in devices])
+        h = ctypes.c_void_p()
+        _check(self.lib.qas_dd_create(ctypes.byref(h), ctypes.byref(g), ctypes.byref(sc), ctypes.byref(b),
+                                      int(nparts), devs), "qas_dd_create")
+        self.h = h
+        self.shape = (8, prob.nz, prob.ny, prob.nx)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.qas_dd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, state: np.ndarray) -> None:
+        a = np.ascontiguousarray(state, dtype=np.float64).reshape(self.shape)
+        _check(self.lib.qas_dd_upload_block(self.h, _dptr(a)), "qas_dd_upload_block")
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        _check(self.lib.qas_dd_download_block(self.h, _dptr(out)), "qas_dd_download_block")
+        return out
+
+    def run(self, max_steps: int = 0, flg: int = 1, stop_rule: int = 0, cfl: float = 0.4, dtrec: float = 1.0,
+            nout: int = 1) -> RunInfo:
+        o = RunOpts(int(max_steps), int(flg), int(stop_rule), float(cfl), float(dtrec), int(nout), 0, 0.0, 0.0)
+        info = RunInfo()
+        _check(self.lib.qas_dd_run(self.h, ctypes.byref(o), ctypes.byref(info)), "qas_dd_run")
+        return info
+
+    def kernel_launches(self):
+        k, c = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self.lib.qas_dd_kernel_launches(self.h, ctypes.byref(k), ctypes.byref(c)), "qas_dd_kernel_launches")
+        return int(k.value), int(c.value)
 
 
 def _grid_scheme_bc(prob):
