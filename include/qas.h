@@ -181,6 +181,18 @@ typedef struct {
 qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, qas_kernel_time *out,
                            int max_entries, int *count);
 
+/* Gravity form of the 2D/3D drivers (2D/SERIAL/RTI, 3D/MPI/RTI: the API's phi_g,
+ * common/mhd_class.hpp:39): phi_g = the gravitational potential of every padded cell (nd
+ * doubles, host, reference layout), copied to the device; NULL switches gravity off.  With it
+ * prmtv and setdt see en - ro*phi_g (and store (en - ro*phi_g) + ro*phi_g back, as the
+ * drivers do), the energy flux carries flux_ro*0.5*(phi_L+phi_R), the momentum update the
+ * source -rk_fac[rk][1]*ro*0.5*(phi(+1)-phi(-1))*dt/dx per axis, and every ghost fill of the
+ * state sets the energy of the last axis' ghost layers from the first/last interior layer
+ * (mhd2d_class.cpp:10-32 / mhd3d_class.cpp:14-40 of those drivers).  The state's en must
+ * already include ro*phi_g, as the drivers' init_ leaves it.  QAS_ERR_UNSUPPORTED in 1D;
+ * the dissipative and adjoint forms refuse a context with gravity (no such driver). */
+qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
+
 /* Tuning options (defaults are the measured best on B200).
  *   QAS_OPT_FUSED_SWEEP: 0 = reconstruction and Riemann flux of each direction in two
  *   kernels with the face states in HBM (default); 1 = one fused sweep kernel.

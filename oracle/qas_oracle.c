@@ -935,6 +935,27 @@ void qo_bound(const qo_grid *g, double *u)
   const int *dn[3] = {g->dnx, g->dny, g->dnz};
   const int *st[3] = {ST_X, ST_Y, ST_Z};
   fill_ghosts(&e, f, 8, dn, st);
+  if (g->phi && g->dim >= 2) {
+    /* gravity drivers: the energy in the ghost layers of the last axis from the first/last
+     * interior layer and the potential difference (2D/SERIAL/RTI/mhd2d_class.cpp:10-32,
+     * 3D/MPI/RTI/mhd3d_class.cpp:14-40) */
+    const double *phi = g->phi;
+    double *ro = f[0], *en = f[7];
+    double fac = (2.0 - g->gam) / (g->gam - 1.0);
+    int n = g->dim == 3 ? e.nz : e.ny;
+    long sl = g->dim == 3 ? e.sz : e.sy;    /* stride of the last axis */
+    long layer = sl;                         /* cells per layer */
+    for (int q = 0; q < GH; q++)
+      for (long c = 0; c < layer; c++) {
+        long ss = (long)q * sl + c, sb = (long)GH * sl + c;
+        en[ss] = en[sb] - fac * ro[sb] * (phi[ss] - phi[sb]);
+      }
+    for (int q = n - GH; q < n; q++)
+      for (long c = 0; c < layer; c++) {
+        long ss = (long)q * sl + c, sb = (long)(n - GH - 1) * sl + c;
+        en[ss] = en[sb] - fac * ro[sb] * (phi[ss] - phi[sb]);
+      }
+  }
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1067,6 +1088,8 @@ static void sweep(const geo *e, const double *const *u, work *w, int axis)
         F[(long)bcomp[1] * nd + ssf] = Fl[4];
         F[(long)bcomp[2] * nd + ssf] = Fl[5];
         F[7 * nd + ssf] = Fl[6];
+        /* work done by gravity (2D/SERIAL/RTI/mhd2d_solve.cpp:197, :305; 3D/MPI/RTI :247, :412, :577) */
+        if (g->phi) F[7 * nd + ssf] += Fl[0] * 0.5 * (g->phi[sl] + g->phi[sr]);
         if (dim >= 2) {
           /* induction fluxes split (2D: only B_b for x, B_a... see below) */
           double q0l, q0r, q1l, q1r, dummy;
@@ -1239,11 +1262,14 @@ static void ideal_stage(const geo *e, double *const *u, work *w, int rk, double 
   /* primitives everywhere: prmtv (common/mhd_class.hpp:80-85) */
 #pragma omp parallel for schedule(static)
   for (ss = 0; ss < nd; ss++) {
+    /* gravity drivers: en -= ro*phi; prmtv; en += ro*phi (2D/SERIAL/RTI/mhd2d_solve.cpp:85-88) */
+    if (g->phi) u[7][ss] -= u[0][ss] * g->phi[ss];
     double iro = 1.0 / u[0][ss];
     w->vx[ss] = u[1][ss] * iro;
     w->vy[ss] = u[2][ss] * iro;
     w->vz[ss] = u[3][ss] * iro;
     w->pr[ss] = ieos(u[0][ss], w->vx[ss], w->vy[ss], w->vz[ss], w->cx[ss], w->cy[ss], w->cz[ss], u[7][ss], g->gam);
+    if (g->phi) u[7][ss] += u[0][ss] * g->phi[ss];
   }
 
   if (dim >= 2) {
@@ -1304,6 +1330,14 @@ static void ideal_stage(const geo *e, double *const *u, work *w, int rk, double 
           int m = cen[c];
           double d = div_flux(e, w, m, ss, dtd, df);
           rk_combine(&u[m][ss], w->ut[(long)m * nd + ss], d, rkf[0], rkf[1]);
+        }
+        if (g->phi) {
+          /* work done by gravity on the momentum, with the updated density
+           * (2D/SERIAL/RTI/mhd2d_solve.cpp:361-362, 3D/MPI/RTI/mhd3d_solve.cpp:679-681) */
+          const double *phi = g->phi;
+          u[1][ss] += -rkf[1] * u[0][ss] * 0.5 * (phi[ss + 1] - phi[ss - 1]) * dtd[0];
+          u[2][ss] += -rkf[1] * u[0][ss] * 0.5 * (phi[ss + sy] - phi[ss - sy]) * dtd[1];
+          if (dim == 3) u[3][ss] += -rkf[1] * u[0][ss] * 0.5 * (phi[ss + sz] - phi[ss - sz]) * dtd[2];
         }
       }
 
@@ -1366,13 +1400,16 @@ int qo_step(const qo_grid *g, double *u, double dt)
   return 0;
 }
 
-/* setdt reduction (mhd1d_class.cpp:11-30, mhd2d_class.cpp:11-33, mhd3d_class.cpp:15-46) */
-double qo_cfl_dt(const qo_grid *g, const double *u, double unused)
+/* setdt reduction (mhd1d_class.cpp:11-30, mhd2d_class.cpp:11-33, mhd3d_class.cpp:15-46; the
+ * gravity drivers' energy rewrite: 2D/SERIAL/RTI/mhd2d_class.cpp:46-48, 3D/MPI/RTI
+ * mhd3d_class.cpp:56-58) */
+double qo_cfl_dt(const qo_grid *g, double *u, double unused)
 {
   (void)unused;
   geo e = mkgeo(g);
   const double *ro = u, *mx = u + e.nd, *my = u + 2 * e.nd, *mz = u + 3 * e.nd;
-  const double *bx = u + 4 * e.nd, *by = u + 5 * e.nd, *bz = u + 6 * e.nd, *en = u + 7 * e.nd;
+  const double *bx = u + 4 * e.nd, *by = u + 5 * e.nd, *bz = u + 6 * e.nd;
+  double *en = u + 7 * e.nd;
   double vmax = 1.0;
   int k0 = g->dim == 3 ? GH : 0, k1 = g->dim == 3 ? e.nz - GH : 1;
   int j0 = g->dim >= 2 ? GH : 0, j1 = g->dim >= 2 ? e.ny - GH : 1;
@@ -1388,9 +1425,11 @@ double qo_cfl_dt(const qo_grid *g, const double *u, double unused)
           cy = 0.5 * (by[ss] + by[ss + e.sy]);
           cz = g->dim == 3 ? 0.5 * (bz[ss] + bz[ss + e.sz]) : bz[ss];
         }
+        if (g->phi) en[ss] -= ro[ss] * g->phi[ss];  /* 2D/SERIAL/RTI/mhd2d_class.cpp:46-48 */
         double iro = 1.0 / ro[ss];
         double vx = mx[ss] * iro, vy = my[ss] * iro, vz = mz[ss] * iro;
         double pr = ieos(ro[ss], vx, vy, vz, cx, cy, cz, en[ss], g->gam);
+        if (g->phi) en[ss] += ro[ss] * g->phi[ss];
         double vf = sqrt((g->gam * pr + (cx * cx + cy * cy + cz * cz)) / ro[ss]);
         double vt;
         if (g->dim == 1)

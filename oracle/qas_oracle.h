@@ -25,6 +25,8 @@ typedef struct {
   int ctw;             /* CUCT upwind weighting on/off */
   double gam, dx, dy, dz;
   int dnx[8], dny[8], dnz[8];   /* boundary flags per field */
+  const double *phi;   /* gravitational potential phi_g (nd doubles), NULL without gravity:
+                          the gravity form of the 2D/3D drivers (2D/SERIAL/RTI, 3D/MPI/RTI) */
 } qo_grid;
 
 /* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,
@@ -37,8 +39,10 @@ int qo_step(const qo_grid *g, double *u, double dt);
 
 /* max(1, max over interior of |v| + c_f), the reduction inside setdt()
  * (mhd1d_class.cpp:11-30, mhd2d_class.cpp:11-33, mhd3d_class.cpp:15-46).  `unused`
- * is ignored (kept for ABI stability of the test binding). */
-double qo_cfl_dt(const qo_grid *g, const double *u, double unused);
+ * is ignored (kept for ABI stability of the test binding).  With gravity the energy of each
+ * interior cell is rewritten as (en - ro*phi) + ro*phi, as the gravity drivers' setdt does
+ * (2D/SERIAL/RTI/mhd2d_class.cpp:46-48). */
+double qo_cfl_dt(const qo_grid *g, double *u, double unused);
 
 /* One visco-resistive stage loop, DMHD2D::dsptv(dt) (2D/SERIAL/MRX/dmhd2d_solve.cpp:3-151)
  * with uniform nu0, eta0.  2D only. */

@@ -12,13 +12,22 @@
  * Test infrastructure only.
  */
 #include <omp.h>
+#ifdef QAS_GRAVITY
+/* gravity form: built against 2D/SERIAL/RTI (MHD2D with phi_g; no dissipative driver) */
+#include "mhd2d_class.hpp"
+typedef MHD2D RefBase;
+#else
 #include "dmhd2d_class.hpp"
+typedef DMHD2D RefBase;
+#endif
 #include "qas_ref_io.h"
 
 int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
 double qh_dtrec = 1.0, qh_cfl = 0.4;
 
 static double g_nu0 = 0.0, g_eta0 = 0.0;
+
+#ifndef QAS_GRAVITY
 
 /* Uniform visco-resistive coefficients; same reduction as the reference's
  * localized-profile version (2D/SERIAL/MRX/dmhd2d_init_.cpp:85-106). */
@@ -37,7 +46,9 @@ double DMHD2D::setdc()
   return dcmax;
 }
 
-class RefHarness2D : public DMHD2D {
+#endif
+
+class RefHarness2D : public RefBase {
  public:
   void setup(const RefCaseHeader &h, const double *data)
   {
@@ -51,9 +62,18 @@ class RefHarness2D : public DMHD2D {
     for (int j = 0; j < ny; j++) y[j] = (j - yoff + 0.5) * dy + ymin;
     for (int m = 0; m < nm; m++) { dnxs[m] = h.dnx[m]; dnys[m] = h.dny[m]; }
     for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nd, sizeof(double) * nd);
+#ifdef QAS_GRAVITY
+    if (!h.has_phi) ref_die("the gravity build needs phi_g in the case");
+    memcpy(phi_g, data + (size_t)8 * nd, sizeof(double) * nd);
+#else
+    if (h.has_phi) ref_die("phi_g given to a build without gravity");
+#endif
   }
   void dissipate()
   {
+#ifdef QAS_GRAVITY
+    ref_die("no dissipative form in the gravity build");
+#else
     double dcmax = setdc();
     if (dcmax > 1e-15) {
       int nc, ncmax = 1 + (int)(2 * (dcmax * dt) / (dr * dr));
@@ -62,6 +82,7 @@ class RefHarness2D : public DMHD2D {
         dsptv(dt / ncmax);
       }
     }
+#endif
   }
   void one_step(int flg, bool resist, std::vector<double> *dts)
   {
@@ -83,11 +104,15 @@ class RefHarness2D : public DMHD2D {
       ideal(dt);
       steps = 1;
     } else if (h.mode == REF_MODE_DSTEP) {
+#ifdef QAS_GRAVITY
+      ref_die("no dissipative form in the gravity build");
+#else
       dt = h.dt;
       dts->push_back(dt);
       setdc();
       bound(val, nm, stxs, dnxs, stys, dnys);
       dsptv(dt);
+#endif
       steps = 1;
     } else if (h.mode == REF_MODE_RUN || h.mode == REF_MODE_DRUN) {
       setdt(1);

@@ -8,13 +8,22 @@
  * without their backup/output side effects.  Test infrastructure only.
  */
 #include <omp.h>
+#ifdef QAS_GRAVITY
+/* gravity form: built against 3D/MPI/RTI (MHD3D with phi_g; no dissipative driver) */
+#include "mhd3d_class.hpp"
+typedef MHD3D RefBase;
+#else
 #include "dmhd3d_class.hpp"
+typedef DMHD3D RefBase;
+#endif
 #include "qas_ref_io.h"
 
 int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
 double qh_dtrec = 1.0, qh_cfl = 0.4;
 
 static double g_nu0 = 0.0, g_eta0 = 0.0;
+
+#ifndef QAS_GRAVITY
 
 /* Uniform visco-resistive coefficients; same reduction as the reference's
  * localized-profile version (3D/MPI/MRX/dmhd3d_init_.cpp:98-127; one rank). */
@@ -35,9 +44,11 @@ double DMHD3D::setdc()
   return dcmax;
 }
 
-class RefHarness3D : public DMHD3D {
+#endif
+
+class RefHarness3D : public RefBase {
  public:
-  RefHarness3D(int *argc, char ***argv) : DMHD3D(argc, argv, 1) {}
+  RefHarness3D(int *argc, char ***argv) : RefBase(argc, argv, 1) {}
   void setup(const RefCaseHeader &h, const double *data)
   {
     setgam(h.gam);
@@ -52,9 +63,18 @@ class RefHarness3D : public DMHD3D {
     for (int k = 0; k < nz; k++) z[k] = (k - zoff + 0.5) * dz + zmin;
     for (int m = 0; m < nm; m++) { dnxs[m] = h.dnx[m]; dnys[m] = h.dny[m]; dnzs[m] = h.dnz[m]; }
     for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nd, sizeof(double) * nd);
+#ifdef QAS_GRAVITY
+    if (!h.has_phi) ref_die("the gravity build needs phi_g in the case");
+    memcpy(phi_g, data + (size_t)8 * nd, sizeof(double) * nd);
+#else
+    if (h.has_phi) ref_die("phi_g given to a build without gravity");
+#endif
   }
   void dissipate()
   {
+#ifdef QAS_GRAVITY
+    ref_die("no dissipative form in the gravity build");
+#else
     double dcmax = setdc();
     if (dcmax > 1e-15) {
       int nc, ncmax = 1 + (int)(2 * (dcmax * dt) / (dr * dr));
@@ -63,6 +83,7 @@ class RefHarness3D : public DMHD3D {
         dsptv(dt / ncmax);
       }
     }
+#endif
   }
   void one_step(int flg, bool resist, std::vector<double> *dts)
   {
@@ -84,11 +105,15 @@ class RefHarness3D : public DMHD3D {
       ideal(dt);
       steps = 1;
     } else if (h.mode == REF_MODE_DSTEP) {
+#ifdef QAS_GRAVITY
+      ref_die("no dissipative form in the gravity build");
+#else
       dt = h.dt;
       dts->push_back(dt);
       setdc();
       bound(val, nm, stxs, dnxs, stys, dnys, stzs, dnzs);
       dsptv(dt);
+#endif
       steps = 1;
     } else if (h.mode == REF_MODE_RUN || h.mode == REF_MODE_DRUN) {
       setdt(1);

@@ -4,7 +4,7 @@
  *
  * Input  : RefCaseHeader, then 8 arrays (ro,mx,my,mz,bx,by,bz,en) of nd doubles,
  *          each in the reference layout ss = nx*(ny*k+j)+i with 4 ghost cells
- *          per side (2D/SERIAL/OTvortex/mhd2d_class.hpp:10-12).
+ *          per side (2D/SERIAL/OTvortex/mhd2d_class.hpp:10-12), then phi_g when has_phi.
  * Output : RefResultHeader, n_dt doubles (dt used by each step), the 8 arrays
  *          after the run, then int32 count + per-step wall times (RUN modes).
  */
@@ -39,7 +39,7 @@ struct RefCaseHeader {
   int32_t dim, nxm, nym, nzm;
   int32_t rmn, odr, rk, ctw;
   int32_t mode, nsteps, flg, nthreads;
-  int32_t nout, pad0;
+  int32_t nout, has_phi;  /* has_phi: nd doubles of phi_g follow the 8 state arrays */
   double gam, cfl, dtrec, dt;
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double nu0, eta0;
@@ -77,7 +77,7 @@ static inline void ref_read_case(const char *path, RefCaseHeader *h, std::vector
   long nx = h->nxm + 8;
   long ny = h->dim >= 2 ? h->nym + 8 : 1;
   long nz = h->dim >= 3 ? h->nzm + 8 : 1;
-  size_t n = (size_t)(8 * nx * ny * nz);
+  size_t n = (size_t)((8 + (h->has_phi ? 1 : 0)) * nx * ny * nz);
   data->resize(n);
   if (fread(data->data(), sizeof(double), n, f) != n) ref_die("short data");
   fclose(f);

@@ -37,13 +37,23 @@ MAGIC_IN = 0x31534151
 MAGIC_OUT = 0x32534151
 
 
-def ref_binary(dim: int, ctw: int) -> str:
-    name = "ref1d" if dim == 1 else f"ref{dim}d_ctw{int(bool(ctw))}"
+def ref_binary(dim: int, ctw: int, gravity: bool = False) -> str:
+    """The reference build for a case: ref1d, ref{2,3}d_ctw*, or the gravity drivers
+    (2D/SERIAL/RTI, 3D/MPI/RTI) ref{2,3}d_g_ctw*."""
+    if dim == 1:
+        name = "ref1d"
+    else:
+        name = f"ref{dim}d_{'g_' if gravity else ''}ctw{int(bool(ctw))}"
     return os.path.join(REF_DIR, name)
 
 
-def reference_available(dim: int = 2, ctw: int = 1) -> bool:
-    return os.access(ref_binary(dim, ctw), os.X_OK)
+def reference_available(dim: int = 2, ctw: int = 1, gravity: bool = False) -> bool:
+    return os.access(ref_binary(dim, ctw, gravity), os.X_OK)
+
+
+def _phi(prob) -> Optional[np.ndarray]:
+    phi = getattr(prob, "phi", None)
+    return None if phi is None else np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
 
 
 def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nthreads: int = 0,
@@ -51,9 +61,10 @@ def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nth
     st = prob.state if state is None else state
     st = np.ascontiguousarray(st, dtype=np.float64).reshape(8, -1)
     assert st.shape[1] == prob.nd, (st.shape, prob.nd)
+    phi = _phi(prob)
     hdr = _HDR.pack(MAGIC_IN, prob.dim, prob.nxm, prob.nym, prob.nzm,
                     prob.rmn, prob.odr, prob.rk, prob.ctw,
-                    mode, nsteps, prob.flg, nthreads, prob.nout, 0,
+                    mode, nsteps, prob.flg, nthreads, prob.nout, 0 if phi is None else 1,
                     prob.gam, prob.cfl, prob.dtrec, dt,
                     prob.xmin, prob.xmax, prob.ymin, prob.ymax, prob.zmin, prob.zmax,
                     prob.nu0, prob.eta0,
@@ -61,6 +72,9 @@ def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nth
     with open(path, "wb") as f:
         f.write(hdr)
         f.write(st.tobytes())
+        if phi is not None:
+            assert phi.size == prob.nd
+            f.write(phi.tobytes())
 
 
 def read_result(path: str, prob):
@@ -85,7 +99,7 @@ def read_result(path: str, prob):
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
                   state: Optional[np.ndarray] = None, timeout: float = 3600.0):
     """Run the reference's own code on ``prob`` and return its result dict."""
-    exe = ref_binary(prob.dim, prob.ctw)
+    exe = ref_binary(prob.dim, prob.ctw, _phi(prob) is not None)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"reference oracle binary missing: {exe} (build with `make -C oracle ref`)")
     with tempfile.TemporaryDirectory(prefix="qasref_") as td:
@@ -187,7 +201,8 @@ class _OGrid(ctypes.Structure):
                 ("rk", ctypes.c_int), ("ctw", ctypes.c_int),
                 ("gam", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double),
-                ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8)]
+                ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8),
+                ("phi", ctypes.POINTER(ctypes.c_double))]
 
 
 class Restatement:
@@ -223,6 +238,10 @@ class Restatement:
         g.dz = prob.dz if prob.dim >= 3 else 0.0
         for m in range(8):
             g.dnx[m], g.dny[m], g.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+        phi = _phi(prob)
+        if phi is not None:
+            g._phi_keep = phi  # the pointer below must outlive the call
+            g.phi = phi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         return g
 
     @staticmethod

@@ -97,6 +97,7 @@ struct qas_ctx {
   // reconstruction with TMA-staged stencils (qas_tma.cuh): per-axis tensor maps, work plan
   // and persistent grid size; lr_tma_ok = supported by this grid, lr_tma = in use
   bool lr_tma_ok = false, lr_tma = false;
+  double *d_phi = nullptr;  // gravitational potential of the gravity drivers (qas_set_gravity)
   LrTmaMaps lr_maps[3];
   LrTmaPlan lr_plan[3];
   int lr_grid[3] = {0, 0, 0};
@@ -799,6 +800,7 @@ qas_status qas_destroy(qas_ctx *c)
   if (c->d_ctl) cudaFree(c->d_ctl);
   if (c->d_dctl) cudaFree(c->d_dctl);
   if (c->d_scratch) cudaFree(c->d_scratch);
+  if (c->d_phi) cudaFree(c->d_phi);
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -926,7 +928,7 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
   qas_run_opts o = *opts;
   if (o.stop_rule < 0 || o.stop_rule > 2) return QAS_ERR_INVALID;
   if (o.stop_rule == 0 && o.max_steps <= 0) return QAS_ERR_INVALID;
-  if ((o.nu0 > 0.0 || o.eta0 > 0.0) && c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
+  if ((o.nu0 > 0.0 || o.eta0 > 0.0) && (c->grid.dim < 2 || c->view.phi)) return QAS_ERR_UNSUPPORTED;
   qas_status s;
   if (!c->run_initialised) {
     // setdt(1) of main(): dt and nmax from the initial state
@@ -1020,7 +1022,7 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
 qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
-  if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
+  if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   const Geo &g = c->geo;
   const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
@@ -1058,7 +1060,7 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
-  if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
+  if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
   c->launches += 1 + launch_dissipate(c, nu0, eta0);
@@ -1168,6 +1170,30 @@ qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas
   }
   *count = w;
   return read_ctl(c);
+}
+
+qas_status qas_set_gravity(qas_ctx *c, const double *phi_g)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->graph) {  // captured launches carry the view by value
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if (!phi_g) {
+    c->view.phi = nullptr;
+    return QAS_OK;
+  }
+  const size_t bytes = (size_t)c->geo.nd * sizeof(double);
+  if (!c->d_phi && cudaMalloc(&c->d_phi, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return QAS_ERR_NOMEM;
+  }
+  QAS_CUDA(cudaMemcpy(c->d_phi, phi_g, bytes, cudaMemcpyHostToDevice));
+  c->view.phi = c->d_phi;
+  c->view.gfac = (2.0 - c->grid.gam) / (c->grid.gam - 1.0);  // fac of the drivers' bound()
+  return QAS_OK;
 }
 
 qas_status qas_set_option(qas_ctx *c, int option, int value)

@@ -64,6 +64,10 @@ struct View {
   Ctl *ctl;
   Maps maps;
   double dr;  // min cell size, the dr of setdt
+  // gravity drivers (2D/SERIAL/RTI, 3D/MPI/RTI): potential phi_g per cell, or null; and
+  // (2-gam)/(gam-1) of their boundary energy rule
+  const double *phi;
+  double gfac;
 };
 
 __device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
@@ -141,13 +145,18 @@ __device__ __forceinline__ void prim_body(const View &v, int i, int j, int k)
     }
   }
   const double ro = v.u[0][c];
+  // gravity drivers: en -= ro*phi; prmtv; en += ro*phi, which leaves en rounded in place
+  // (2D/SERIAL/RTI/mhd2d_solve.cpp:85-88, 3D/MPI/RTI/mhd3d_solve.cpp:95-97)
+  double en = v.u[7][c];
+  if (v.phi) en = en - ro * v.phi[c];
   const double iro = 1.0 / ro;
   const double vx = v.u[1][c] * iro;
   const double vy = v.u[2][c] * iro;
   const double vz = v.u[3][c] * iro;
   const double v2 = vx * vx + vy * vy + vz * vz;
   const double b2 = cx * cx + cy * cy + cz * cz;
-  const double pr = (v.gam - 1) * (v.u[7][c] - 0.5 * (ro * v2 + b2));
+  const double pr = (v.gam - 1) * (en - 0.5 * (ro * v2 + b2));
+  if (v.phi) v.u[7][c] = en + ro * v.phi[c];
   v.vx[c] = vx;
   v.vy[c] = vy;
   v.vz[c] = vz;
@@ -337,7 +346,8 @@ __device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
   }
   v.f[A][4 + B][f] = fbt;
   v.f[A][4 + C][f] = fbu;
-  v.f[A][7][f] = F[6];
+  // work done by gravity (2D/SERIAL/RTI/mhd2d_solve.cpp:197, :305; 3D/MPI/RTI/mhd3d_solve.cpp:247, :412, :577)
+  v.f[A][7][f] = v.phi ? F[6] + F[0] * 0.5 * (v.phi[f - s] + v.phi[f]) : F[6];
 }
 template <int RMN, int A>
 __global__ void __launch_bounds__(128) k_flux(View v)
@@ -444,7 +454,7 @@ __device__ __forceinline__ void face_flux(const View &v, long long f, const doub
   }
   v.f[A][4 + B][f] = fbt;
   v.f[A][4 + C][f] = fbu;
-  v.f[A][7][f] = F[6];
+  v.f[A][7][f] = v.phi ? F[6] + F[0] * 0.5 * (__ldg(v.phi + f - s) + __ldg(v.phi + f)) : F[6];
 }
 
 // x sweep: 4 warps per block, 31 faces per warp
@@ -627,6 +637,14 @@ __device__ __forceinline__ void update_body(const View &v, int i, int j, int k, 
       nv[m] = rk_combine(v.u[m][c], v.u0[m][c], du, c0, c1);
       wr[m] = true;
     }
+    if (v.phi) {
+      // work done by gravity on the momentum, with the updated density (2D/SERIAL/RTI/
+      // mhd2d_solve.cpp:361-362, 3D/MPI/RTI/mhd3d_solve.cpp:679-681)
+      const double *ph = v.phi;
+      nv[1] = nv[1] + -c1 * nv[0] * 0.5 * (ph[c + 1] - ph[c - 1]) * dtdx;
+      nv[2] = nv[2] + -c1 * nv[0] * 0.5 * (ph[c + sy] - ph[c - sy]) * dtdy;
+      if (g.dim == 3) nv[3] = nv[3] + -c1 * nv[0] * 0.5 * (ph[c + sz] - ph[c - sz]) * dtdz;
+    }
   }
   if (g.dim == 2) {
     if (cj) {  // bx on i in [GH, nx-GH]
@@ -752,6 +770,24 @@ __device__ __forceinline__ void bound_body(const View &v, int i, int j, int k)
     wr[m] = si != i || sj != j || sk != k;
     nv[m] = wr[m] ? fac * v.u[m][cidx(g, si, sj, sk)] : 0.0;
   }
+  if (v.phi && g.dim >= 2) {
+    // gravity drivers: the energy of the ghost layers of the last axis from the filled first /
+    // last interior layer (2D/SERIAL/RTI/mhd2d_class.cpp:10-32, 3D/MPI/RTI/mhd3d_class.cpp:14-40)
+    const int h = g.dim == 3 ? k : j, n = g.dim == 3 ? g.nz : g.ny;
+    if (h < GH || h >= n - GH) {
+      const int hb = h < GH ? GH : n - GH - 1;
+      const int bj = g.dim == 3 ? j : hb, bk = g.dim == 3 ? hb : k;
+      int si, sj, sk;
+      double fr, fe;
+      gather_src(v, 0, 0, i, bj, bk, si, sj, sk, fr);
+      const double ro_b = fr * v.u[0][cidx(g, si, sj, sk)];
+      gather_src(v, 0, 7, i, bj, bk, si, sj, sk, fe);
+      const double en_b = fe * v.u[7][cidx(g, si, sj, sk)];
+      const long long b = cidx(g, i, bj, bk);
+      nv[7] = en_b - v.gfac * ro_b * (v.phi[c] - v.phi[b]);
+      wr[7] = true;
+    }
+  }
 #pragma unroll
   for (int m = 0; m < 8; m++)
     if (wr[m]) v.u[m][c] = nv[m];
@@ -824,7 +860,12 @@ __device__ __forceinline__ double vmax_cell(const View &v, int i, int j, int k)
     const double vx = v.u[1][c] * iro, vy = v.u[2][c] * iro, vz = v.u[3][c] * iro;
     const double v2 = vx * vx + vy * vy + vz * vz;
     const double b2 = cx * cx + cy * cy + cz * cz;
-    const double pr = (v.gam - 1) * (v.u[7][c] - 0.5 * (ro * v2 + b2));
+    // gravity drivers' setdt: the same en -= ro*phi; prmtv; en += ro*phi on the interior
+    // (2D/SERIAL/RTI/mhd2d_class.cpp:46-48, 3D/MPI/RTI/mhd3d_class.cpp:56-58)
+    double en = v.u[7][c];
+    if (v.phi) en = en - ro * v.phi[c];
+    const double pr = (v.gam - 1) * (en - 0.5 * (ro * v2 + b2));
+    if (v.phi) v.u[7][c] = en + ro * v.phi[c];
     const double vf = sqrt((v.gam * pr + (cx * cx + cy * cy + cz * cz)) / ro);
     double vt;
     if (g.dim == 1)

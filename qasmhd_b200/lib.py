@@ -38,7 +38,7 @@ EXPORTS = (
     "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
     "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
     "qas_bkup_load", "qas_dd_plan", "qas_dd_create", "qas_dd_destroy", "qas_dd_upload_block",
-    "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches",
+    "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches", "qas_set_gravity",
 )
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
@@ -166,6 +166,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_dd_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(Grid), ctypes.POINTER(Scheme),
                                   ctypes.POINTER(BC), ctypes.c_int, ip]
     lib.qas_dd_destroy.argtypes = [vp]
+    lib.qas_set_gravity.argtypes = [vp, dp]
     lib.qas_dd_upload_block.argtypes = [vp, dp]
     lib.qas_dd_download_block.argtypes = [vp, dp]
     lib.qas_dd_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
@@ -214,9 +215,23 @@ class Context:
 
     @classmethod
     def from_problem(cls, prob, device: int = -1) -> "Context":
-        return cls(prob.dim, prob.nxm, prob.nym, prob.nzm, prob.dx, prob.dy if prob.dim >= 2 else 0.0,
-                   prob.dz if prob.dim >= 3 else 0.0, prob.gam, prob.rmn, prob.odr, prob.rk, prob.ctw,
-                   prob.dnx, prob.dny, prob.dnz, device)
+        """A context for the problem; with gravity (prob.phi) the gravity form is switched on."""
+        ctx = cls(prob.dim, prob.nxm, prob.nym, prob.nzm, prob.dx, prob.dy if prob.dim >= 2 else 0.0,
+                  prob.dz if prob.dim >= 3 else 0.0, prob.gam, prob.rmn, prob.odr, prob.rk, prob.ctw,
+                  prob.dnx, prob.dny, prob.dnz, device)
+        if getattr(prob, "phi", None) is not None:
+            ctx.set_gravity(prob.phi)
+        return ctx
+
+    def set_gravity(self, phi: Optional[np.ndarray]) -> None:
+        """qas_set_gravity: the gravitational potential of every padded cell, or None (off)."""
+        if phi is None:
+            _check(self.lib.qas_set_gravity(self.h, None), "qas_set_gravity")
+            return
+        a = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+        if a.size != self.nd:
+            raise ValueError(f"phi has {a.size} values, the grid {self.nd}")
+        _check(self.lib.qas_set_gravity(self.h, _dptr(a)), "qas_set_gravity")
 
     def close(self) -> None:
         if getattr(self, "h", None):

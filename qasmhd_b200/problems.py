@@ -60,6 +60,8 @@ class Problem:
     # exec_ flag: 1 = dt refreshed every 2nd step (2D/3D drivers), 0 = constant dt (1D driver)
     flg: int = 1
     state: Optional[np.ndarray] = None  # shape (8, nz, ny, nx) incl. ghosts
+    # gravitational potential phi_g (nz, ny, nx) of the gravity drivers, None without gravity
+    phi: Optional[np.ndarray] = None
 
     @property
     def nx(self) -> int:
@@ -108,6 +110,7 @@ class Problem:
     def copy(self) -> "Problem":
         p = dataclasses.replace(self)
         p.state = None if self.state is None else self.state.copy()
+        p.phi = None if self.phi is None else self.phi.copy()
         return p
 
 
@@ -297,6 +300,77 @@ def smooth_wave(dim: int, n: int, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3
 # ----------------------------------------------------------------------------
 # C4: batched ensemble
 # ----------------------------------------------------------------------------
+
+def rayleigh_taylor(dim: int = 2, nxm: int = 128, ngm: int = 1024, nym3: Optional[int] = None,
+                    rmn: int = RMN_LHLLD, odr: int = 4, rk: int = 3, ctw: int = 1, gam: float = 5.0 / 3.0,
+                    tmax: float = 1e30, nout: int = 1) -> Problem:
+    """Rayleigh-Taylor instability of the gravity drivers (2D/SERIAL/RTI, 3D/MPI/RTI).
+
+    Gravity along the last axis h (y in 2D, z in 3D) from phi_g = g0*lg*log(cosh(h/lg)), g0 = 1,
+    lg = 8 cells; a heavy layer (ro 1) above |h| = 0.35 L_h over a light one (ro 0.1 in 2D,
+    0.2 in 3D), tanh-smoothed over width 1; pressure from the hydrostatic balance
+    dP/dh = -ro dphi/dh integrated from h = 0 (base 500 in 2D, 50 in 3D) by the midpoint rule
+    with 1 + round(|h|/dh) intervals, floored at 1e-4; a uniform field transverse to gravity
+    (bz in 2D, by in 3D) at plasma beta 1e3 (2D) / 1e2 (3D); a single-mode velocity kick of
+    amplitude 0.01 along h localised at the two interfaces.  Box: x (and y in 3D) in [0, 20],
+    h in [-10 ngm/nxm, +10 ngm/nxm]; periodic across, open (+2) along h.  The total energy
+    carries ro*phi_g, as the drivers' init_ does (2D/SERIAL/RTI/mhd2d_init_.cpp:8-88).
+    """
+    if dim not in (2, 3):
+        raise ValueError("the gravity drivers are 2D and 3D")
+    nym = (nxm if nym3 is None else nym3) if dim == 3 else ngm
+    nzm = ngm if dim == 3 else 1
+    hext = 0.5 * 20.0 * ngm / nxm
+    kw = dict(xmin=0.0, xmax=20.0)
+    if dim == 2:
+        kw.update(ymin=-hext, ymax=hext)
+        dn = dict(dnx=(0,) * NM, dny=(2,) * NM, dnz=(0,) * NM)
+    else:
+        kw.update(ymin=0.0, ymax=20.0, zmin=-hext, zmax=hext)
+        dn = dict(dnx=(0,) * NM, dny=(0,) * NM, dnz=(2,) * NM)
+    p = Problem(name=f"rt{dim}d_{nxm}x{ngm}", dim=dim, nxm=nxm, nym=nym, nzm=nzm, rmn=rmn, odr=odr, rk=rk,
+                ctw=ctw, gam=gam, cfl=0.4, dtrec=tmax, nout=nout, flg=1, **kw, **dn)
+    x, y, z = p.coords()
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    H = Y if dim == 2 else Z
+    dh = p.dy if dim == 2 else p.dz
+    lh = p.ymax - p.ymin if dim == 2 else p.zmax - p.zmin
+    g0, lg, width, s0 = 1.0, 8.0 * dh, 1.0, 0.35 * lh
+    ro_u, ro_l = 1.0, (0.1 if dim == 2 else 0.2)
+    pr0, beta = (500.0, 1e3) if dim == 2 else (50.0, 1e2)
+    b0 = math.sqrt(2.0 * pr0 / beta)
+
+    def layer(vu, vl, h):
+        return 0.5 * (2.0 + np.tanh((h - s0) / width) - np.tanh((h + s0) / width)) * (vu - vl) + vl
+
+    def pressure(h):
+        n = 1 + int(abs(h) / dh + 0.5)
+        d = h / n
+        acc = pr0
+        for q in range(n):
+            hc = (q + 0.5) * d
+            acc += -layer(ro_u, ro_l, hc) * (g0 * math.tanh(hc / lg)) * d
+        return acc
+
+    hs = y if dim == 2 else z
+    pr_h = np.array([max(pressure(h), 1e-4) for h in hs])
+    pr = pr_h[None, :, None] if dim == 2 else pr_h[:, None, None]
+    pr = np.broadcast_to(pr, X.shape).astype(np.float64)
+    ro = layer(ro_u, ro_l, H)
+    kick = 0.01 * np.cos(2 * math.pi * X / 20.0) * (1.0 if dim == 2 else np.cos(2 * math.pi * Y / 20.0))
+    vh = kick * (np.exp(-((H - s0) ** 2) / (4 * width ** 2)) - np.exp(-((H + s0) ** 2) / (4 * width ** 2)))
+    zero = np.zeros_like(X)
+    vx, vy, vz = (zero, vh, zero) if dim == 2 else (zero, zero, vh)
+    bx = zero
+    by = zero if dim == 2 else np.full_like(X, b0)
+    bz = np.full_like(X, b0) if dim == 2 else zero
+    phi = g0 * lg * np.log(np.cosh(H / lg))
+    st = _pack(ro, vx, vy, vz, bx, by, bz, pr, bx, by, bz, gam)
+    st[7] = st[7] + ro * phi
+    p.state = st
+    p.phi = phi
+    return p
+
 
 def ensemble(n: int = 512, lo: int = 64, hi: int = 512, seed: int = 2025, odr: int = 4) -> list:
     """Seeded ensemble of 2D instances with log-uniform sides in [lo, hi]

@@ -115,6 +115,9 @@ STEP_CASES = [
     ("kh2d_roe_eta", _kh2_eta, R.MODE_DRUN, 3),
     ("wave3d_eta_ctw1", lambda: _wave3_eta(1, 0.02, 0.05), R.MODE_DRUN, 2),
     ("wave3d_eta_ctw0_sub2", lambda: _wave3_eta(0, 0.05, 0.3, rmn=P.RMN_ROE), R.MODE_DRUN, 2),
+    ("rt2d_lhlld", lambda: P.rayleigh_taylor(2, 16, 32), R.MODE_RUN, 3),
+    ("rt2d_mlau_exec", lambda: P.rayleigh_taylor(2, 16, 32, rmn=P.RMN_MLAU, tmax=0.03), R.MODE_EXEC, 0),
+    ("rt3d_hlld_ctw0", lambda: P.rayleigh_taylor(3, 8, 16, rmn=P.RMN_HLLD, ctw=0), R.MODE_RUN, 2),
     *[(f"kh3d_rmn{r}", (lambda r=r: P.kelvin_helmholtz(3, 6, mach=0.3, rmn=r)), R.MODE_RUN, 2) for r in range(4)],
     *[(f"wave{d}d_bc{s}", (lambda d=d, s=s: _wave_bc(d, s)), R.MODE_RUN, 2) for d in (1, 2, 3) for s in (1, 2)],
 ]

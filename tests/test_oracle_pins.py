@@ -79,3 +79,20 @@ def test_live_reference_dissipative_3d(restatement, ctw):
     a = R.run_reference(p, R.MODE_DRUN, nsteps=2, nthreads=2)
     b = restatement.run(p, 2, mode=R.MODE_DRUN)
     assert_bitwise(b["state"], a["state"], "drun3d")
+
+
+@pytest.mark.skipif(not all(R.reference_available(d, c, gravity=True) for d in (2, 3) for c in (0, 1)),
+                    reason="reference gravity builds not built")
+@pytest.mark.parametrize("dim,ctw,rmn", [(2, 1, P.RMN_LHLLD), (2, 0, P.RMN_ROE), (3, 1, P.RMN_MLAU),
+                                         (3, 0, P.RMN_HLLD)])
+def test_live_reference_gravity(restatement, dim, ctw, rmn):
+    """The gravity drivers (2D/SERIAL/RTI, 3D/MPI/RTI): prmtv/setdt energy shift, gravity work
+    in the energy flux and the momentum update, the ghost-layer energy rule of bound()."""
+    p = P.rayleigh_taylor(dim, 16 if dim == 2 else 8, 32 if dim == 2 else 16, rmn=rmn, ctw=ctw)
+    a = R.run_reference(p, R.MODE_RUN, nsteps=3, nthreads=2)
+    b = restatement.run(p, 3, mode=R.MODE_RUN)
+    assert_bitwise(b["state"], a["state"], f"rt{dim}d")
+    assert np.array_equal(a["dts"], b["dts"])
+    a = R.run_reference(p, R.MODE_STEP, dt=1e-3, nthreads=2)
+    b = restatement.run(p, 1, mode=R.MODE_STEP, dt=1e-3)
+    assert_bitwise(b["state"], a["state"], f"rt{dim}d step")

@@ -275,3 +275,44 @@ def test_tma_staging_unsupported_on_odd_extent():
             ctx.set_option(L.QAS_OPT_LR_STAGING, 1)
         assert e.value.status == L.QAS_ERR_UNSUPPORTED
         ctx.set_option(L.QAS_OPT_LR_STAGING, 0)
+
+
+@pytest.mark.parametrize("dim,rmn,ctw", [(2, P.RMN_LHLLD, 1), (2, P.RMN_HLLD, 0), (3, P.RMN_MLAU, 1),
+                                         (3, P.RMN_ROE, 0)])
+def test_gravity_vs_oracle(restatement, dim, rmn, ctw):
+    """Gravity drivers (2D/SERIAL/RTI, 3D/MPI/RTI) through qas_set_gravity."""
+    p = P.rayleigh_taylor(dim, 64 if dim == 2 else 16, 128 if dim == 2 else 32, rmn=rmn, ctw=ctw)
+    a = restatement.run(p, 6, mode=R.MODE_RUN)
+    b = run_gpu(p, R.MODE_RUN, 6)
+    assert_bitwise(b["state"], a["state"], f"rt{dim}d rmn{rmn}")
+    assert b["steps"] == 6
+
+
+def test_gravity_forms_and_switch(restatement):
+    """Graph, eager, fused sweep and TMA-staged reconstruction agree with gravity on; switching
+    gravity off gives the plain driver; the dissipative form refuses a gravity context."""
+    p = P.rayleigh_taylor(2, 64, 128)
+    ref = restatement.run(p, 4, mode=R.MODE_RUN)["state"]
+    outs = []
+    for opt, val, graph in ((None, 0, True), (None, 0, False), (L.QAS_OPT_FUSED_SWEEP, 1, False),
+                            (L.QAS_OPT_LR_STAGING, 1, True)):
+        with L.Context.from_problem(p) as ctx:
+            if opt is not None:
+                ctx.set_option(opt, val)
+            ctx.upload(p.state)
+            ctx.run(max_steps=4, flg=1, stop_rule=0, cfl=p.cfl, use_graph=graph)
+            outs.append(ctx.download(p.state.shape))
+    for o in outs:
+        assert_bitwise(o, ref, "gravity form")
+    plain = p.copy()
+    plain.phi = None
+    a = restatement.run(plain, 3, mode=R.MODE_RUN)["state"]
+    with L.Context.from_problem(p) as ctx:
+        ctx.set_gravity(None)
+        ctx.upload(p.state)
+        ctx.run(max_steps=3, flg=1, stop_rule=0, cfl=p.cfl)
+        assert_bitwise(ctx.download(p.state.shape), a, "gravity off")
+        ctx.set_gravity(p.phi)
+        with pytest.raises(L.QasError) as e:
+            ctx.dissipate(1e-3, 0.0, 1e-3)
+        assert e.value.status == L.QAS_ERR_UNSUPPORTED
