@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-plain3d", action="store_true",
+                    help="skip the 3D Kelvin-Helmholtz 256^3 leg (GPU vs the reference's OpenMP build)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint comparison over --steps steps (profiling aid)")
     ap.add_argument("--ensemble-only", action="store_true",
@@ -215,6 +217,41 @@ def ensemble_compare(steps):
             "batched_launches": launches_b, "per_instance_launches": launches_p,
             "basis": "ratio: per-instance runs each with its own graph-captured exec_ loop (the strict "
                      "baseline); ratio_vs_eager: per-instance plain (eager) kernel launches"}
+
+
+def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
+    """3D low-Mach Kelvin-Helmholtz 256^3 (MLAU, WCNS4, CUCT, RK3): device-timed throughput of
+    the graph-captured exec_ loop next to the reference's own OpenMP build on all host cores
+    (a bounded sample of full steps)."""
+    import torch
+
+    from qasmhd_b200 import lib as L
+    from qasmhd_b200 import problems as P
+    prob = P.kelvin_helmholtz(3, 256)
+    with L.Context.from_problem(prob) as ctx:
+        ctx.upload(prob.state)
+        ctx.run(max_steps=warmup, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+        ext = torch.cuda.ExternalStream(ctx.stream())
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        ctx.run(max_steps=steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+        b.record(ext)
+        b.synchronize()
+        ms = a.elapsed_time(b) / steps
+        prof = ctx.profile(2, flg=1, cfl=prob.cfl)
+    gpu = prob.interior_cells / (ms * 1e-3) / 1e6
+    cpu = cpu_baseline(prob, steps=cpu_steps) if cpu_steps > 0 else None
+    out = {"workload": "kelvin_helmholtz_3d_256^3_M0.01_mlau_wcns4_ct_rk3", "value": gpu,
+           "unit": "Mcell-updates/s", "ms_per_step": ms, "steps": steps,
+           "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
+           "cpu_baseline": cpu,
+           "step_roofline": {"achieved": ALG_BYTES_PER_CELL_UPDATE * prob.interior_cells / (ms * 1e-3) / 1e9,
+                             "unit": "GB/s", "basis": "512 algorithmic B per cell-update"}}
+    if cpu:
+        out["ratio_vs_cpu"] = gpu / cpu["value"]
+    return out
 
 
 def adjoint_compare(nsteps=400, every=20, eta=0.5e-4):
@@ -430,6 +467,9 @@ def main():
     if rank == 0 and not args.no_adjoint and world == 1:
         ctx.close()
         line["adjoint"] = adjoint_compare()
+    if rank == 0 and not args.no_plain3d and world == 1 and args.workload != "kh3d_256":
+        ctx.close()
+        line["plain3d"] = plain3d_compare(cpu_steps=0 if args.no_cpu_baseline else 2)
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -181,6 +181,17 @@ typedef struct {
 qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, qas_kernel_time *out,
                            int max_entries, int *count);
 
+/* Hall form of the 1D driver (1D/SERIAL/h-shock, HMHD1D): di = ion inertia length, de = the
+ * "artificial" electron inertia length (absolute).  Each exec_ step then runs
+ * hmax = 1 + (int)(dt/haldt) Hall sub-cycles hall_(dt/hmax), each followed by bound(),
+ * between the ghost fill and ideal(dt) (hmhd1d_class.cpp:15-44; haldt: :3-13), with
+ * vphix = di*pi/dx (hmhd1d_paras.cpp:29-34).  The sub-cycle count is read back each step, so
+ * qas_run runs such a context without graph capture.  QAS_ERR_UNSUPPORTED for dim != 1 and for
+ * de != 0 (the electron-inertia correction solve, hmhd1d_solve.cpp:266-426, is not built).
+ * qas_hall: one hall_(dt) call (no ghost fill before), QAS_ERR_UNSUPPORTED without the Hall form. */
+qas_status qas_set_hall(qas_ctx *ctx, double di, double de);
+qas_status qas_hall(qas_ctx *ctx, double dt);
+
 /* Gravity form of the 2D/3D drivers (2D/SERIAL/RTI, 3D/MPI/RTI: the API's phi_g,
  * common/mhd_class.hpp:39): phi_g = the gravitational potential of every padded cell (nd
  * doubles, host, reference layout), copied to the device; NULL switches gravity off.  With it

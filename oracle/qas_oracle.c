@@ -1761,6 +1761,111 @@ int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0
 }
 
 /* ------------------------------------------------------------------------ */
+/* Hall term of the 1D Hall driver: 1D/SERIAL/h-shock/hmhd1d_solve.cpp:138-264 */
+/* ------------------------------------------------------------------------ */
+
+/* HMHD1D::hallv (hmhd1d_class.hpp:28-35) with rotc (common/common_interp.h:39-43) on the
+ * cell-centre field, which is the state's own B in 1D */
+static void hall_velocity(const double *ro, const double *bx, const double *by, const double *bz, double di,
+                          double idx, long i, double *hx, double *hy, double *hz)
+{
+  double fac = di / ro[i];
+  hx[i] = 0.0;
+  hy[i] = -fac * (0.5 * ((bx[i + 0] - bx[i - 0]) * 0.0 - (bz[i + 1] - bz[i - 1]) * idx));
+  hz[i] = -fac * (0.5 * ((by[i + 1] - by[i - 1]) * idx - (bx[i + 0] - bx[i - 0]) * 0.0));
+}
+
+double qo_haldt(const qo_grid *g, const double *u, double cfl, double di, double vphix)
+{
+  geo e = mkgeo(g);
+  long nx = e.nx;
+  const double *ro = u, *bx = u + 4 * nx, *by = u + 5 * nx, *bz = u + 6 * nx;
+  double *h = xcalloc(3 * nx);
+  if (!h) return -1.0;
+  double idx = 1.0 / g->dx, vmax = 1.0;
+  for (long i = GH; i < nx - GH; i++) {
+    hall_velocity(ro, bx, by, bz, di, idx, i, h, h + nx, h + 2 * nx);
+    double vt = fabs(h[i]) + vphix * fabs(bx[i] / ro[i]);
+    if (vt > vmax) vmax = vt;
+  }
+  free(h);
+  return cfl * g->dx / vmax;
+}
+
+/* Lax-Friedrichs Hall flux: calc_flux_hall_lf (common/mhd_flux.c:784-813) */
+static void flux_hall_lf(const double *L, const double *R, double bnc, double smax, double *fbt, double *fbu,
+                         double *fen)
+{
+  double pml = 0.5 * (bnc * bnc + L[4] * L[4] + L[5] * L[5]);
+  double vbl = L[1] * bnc + L[2] * L[4] + L[3] * L[5];
+  double pmr = 0.5 * (bnc * bnc + R[4] * R[4] + R[5] * R[5]);
+  double vbr = R[1] * bnc + R[2] * R[4] + R[3] * R[5];
+  double fbtl = L[4] * L[1] - bnc * L[2];
+  double fbul = L[5] * L[1] - bnc * L[3];
+  double fenl = 2.0 * pml * L[1] - bnc * vbl;
+  double fbtr = R[4] * R[1] - bnc * R[2];
+  double fbur = R[5] * R[1] - bnc * R[3];
+  double fenr = 2.0 * pmr * R[1] - bnc * vbr;
+  *fbt = 0.5 * (fbtl + fbtr - smax * (R[4] - L[4]));
+  *fbu = 0.5 * (fbul + fbur - smax * (R[5] - L[5]));
+  *fen = 0.5 * (fenl + fenr - smax * (pmr - pml));
+}
+
+int qo_hall(const qo_grid *g, double *u, double dt, double di, double vphix)
+{
+  if (g->dim != 1) return -1;
+  geo e = mkgeo(g);
+  long nx = e.nx, i;
+  double *f[8];
+  for (int m = 0; m < 8; m++) f[m] = u + (long)m * nx;
+  double *ut = xcalloc(8 * nx), *h = xcalloc(3 * nx), *vl = xcalloc(7 * nx), *vr = xcalloc(7 * nx);
+  double *fx = xcalloc(3 * nx);
+  if (!ut || !h || !vl || !vr || !fx) return -1;
+  double *hv[3] = {h, h + nx, h + 2 * nx};
+  memcpy(ut, u, sizeof(double) * 8 * nx);
+  lr_fn lr = nl_interp(g->odr);
+  pt_fn df = first_diff(g->odr);
+  double idx = 1.0 / g->dx, dtdx = dt / g->dx;
+  for (int rk = 0; rk < g->rk; rk++) {
+    const double *rkf = RKF[g->rk - 1][rk];
+    for (i = 1; i < nx - 1; i++) hall_velocity(f[0], f[4], f[5], f[6], di, idx, i, hv[0], hv[1], hv[2]);
+    {  /* bound(pv,3,&dnxs[1]) */
+      const int *dn[3] = {g->dnx + 1, g->dny + 1, g->dnz + 1};
+      const int *st[3] = {ST_0, ST_0, ST_0};
+      fill_ghosts(&e, hv, 3, dn, st);
+    }
+    /* mhd_lr_single of ro, hx, hy, hz, by, bz, en: left state at face i+1, right at face i */
+    const double *q[7] = {f[0], hv[0], hv[1], hv[2], f[5], f[6], f[7]};
+    for (i = 2; i < nx - 2; i++)
+      for (int m = 0; m < 7; m++) {
+        double s5[5] = {q[m][i - 2], q[m][i - 1], q[m][i], q[m][i + 1], q[m][i + 2]};
+        lr(&s5[2], &vl[(long)m * nx + i + 1], &vr[(long)m * nx + i]);
+      }
+    for (i = 3; i < nx - 2; i++) {
+      double L[7], R[7];
+      for (int m = 0; m < 7; m++) { L[m] = vl[(long)m * nx + i]; R[m] = vr[(long)m * nx + i]; }
+      double bn = 0.5 * (f[4][i] + f[4][i]);
+      double rn = qmin(L[0], R[0]);
+      double smax = 0.0;
+      smax += qmax(fabs(L[1]), fabs(R[1]));
+      smax += vphix * fabs(bn / rn);
+      flux_hall_lf(L, R, bn, smax, &fx[i], &fx[nx + i], &fx[2 * nx + i]);
+    }
+    /* update of by, bz, en (mhd_updt1d) */
+    for (i = GH; i < nx - GH; i++) {
+      const int mm[3] = {5, 6, 7};
+      for (int c = 0; c < 3; c++) {
+        double d = -dtdx * d4(fx + (long)c * nx, i, 1, df);
+        rk_combine(&f[mm[c]][i], ut[(long)mm[c] * nx + i], d, rkf[0], rkf[1]);
+      }
+    }
+    qo_bound(g, u);
+  }
+  free(ut); free(h); free(vl); free(vr); free(fx);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* known-answer entry (layouts of oracle/ref_harness/ref_kat.cpp)            */
 /* ------------------------------------------------------------------------ */
 int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out)

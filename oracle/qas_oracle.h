@@ -51,6 +51,13 @@ int qo_dsptv(const qo_grid *g, double *u, double dt, double nu0, double eta0);
 /* setdc() + sub-cycled dsptv (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26) with uniform nu0, eta0. */
 int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0);
 
+/* Hall term of the 1D Hall driver (1D/SERIAL/h-shock): one hall_(dt) call
+ * (hmhd1d_solve.cpp:138-264) with ion inertia length di and whistler speed factor vphix and
+ * no electron inertia (de = 0), and haldt() (hmhd1d_class.cpp:3-13), which returns the
+ * Hall sub-cycle time step cfl*dx/max(1, max_i |hx| + vphix |bx/ro|). */
+int qo_hall(const qo_grid *g, double *u, double dt, double di, double vphix);
+double qo_haldt(const qo_grid *g, const double *u, double cfl, double di, double vphix);
+
 /* Point-function known answers; same function ids and layouts as oracle/ref_harness/ref_kat.cpp. */
 int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out);
 

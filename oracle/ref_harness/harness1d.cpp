@@ -6,13 +6,22 @@
  * from the first setdt(1) and nmax = nrec*nout steps.  Test infrastructure only.
  */
 #include <omp.h>
+#ifdef QAS_HALL
+/* Hall form: built against 1D/SERIAL/h-shock (HMHD1D: hmhd1d_class.cpp, hmhd1d_solve.cpp),
+ * with the Hall parameters taken from the case (di = nu0, de = eta0 fields) and vphix set as
+ * HMHD1D::paras does (1D/SERIAL/h-shock/hmhd1d_paras.cpp:29-34). */
+#include "hmhd1d_class.hpp"
+typedef HMHD1D RefBase;
+#else
 #include "mhd1d_class.hpp"
+typedef MHD1D RefBase;
+#endif
 #include "qas_ref_io.h"
 
 int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 4, qh_rk = 3;
 double qh_dtrec = 1.0, qh_cfl = 0.4;
 
-class RefHarness1D : public MHD1D {
+class RefHarness1D : public RefBase {
  public:
   void setup(const RefCaseHeader &h, const double *data)
   {
@@ -23,12 +32,30 @@ class RefHarness1D : public MHD1D {
     for (int i = 0; i < nx; i++) x[i] = (i - xoff + 0.5) * dx + xmin;
     for (int m = 0; m < nm; m++) dnxs[m] = h.dnx[m];
     for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nx, sizeof(double) * nx);
+#ifdef QAS_HALL
+    di = h.nu0;
+    de = h.eta0;
+    idx = 1.0 / dx;
+    double kpeak = M_PI * idx;
+    if (de != 0) kpeak = min(kpeak, 1.0 / de);
+    vphix = di * kpeak;
+#endif
   }
   void one_step(int flg, std::vector<double> *dts)
   {
     tim += dt;
     dts->push_back(dt);
     bound(val, nm, dnxs);
+#ifdef QAS_HALL
+    /* Hall sub-cycles of HMHD1D::exec_ (1D/SERIAL/h-shock/hmhd1d_class.cpp:26-33) */
+    if (di != 0) {
+      int hmax = 1 + (int)(dt / haldt());
+      for (int hs = 0; hs < hmax; hs++) {
+        hall_(dt / hmax);
+        bound(val, nm, dnxs);
+      }
+    }
+#endif
     ideal(dt);
     setdt(flg * (n % 2 == 0));
   }
@@ -42,6 +69,14 @@ class RefHarness1D : public MHD1D {
       bound(val, nm, dnxs);
       ideal(dt);
       steps = 1;
+#ifdef QAS_HALL
+    } else if (h.mode == REF_MODE_DSTEP) {  /* Hall build: bound; one hall_(dt) */
+      dt = h.dt;
+      dts->push_back(dt);
+      bound(val, nm, dnxs);
+      hall_(dt);
+      steps = 1;
+#endif
     } else if (h.mode == REF_MODE_RUN) {
       setdt(1);
       for (int s = 0; s < h.nsteps; s++) {

@@ -41,7 +41,7 @@ def ref_binary(dim: int, ctw: int, gravity: bool = False) -> str:
     """The reference build for a case: ref1d, ref{2,3}d_ctw*, or the gravity drivers
     (2D/SERIAL/RTI, 3D/MPI/RTI) ref{2,3}d_g_ctw*."""
     if dim == 1:
-        name = "ref1d"
+        name = "ref1d_hall" if gravity == "hall" else "ref1d"
     else:
         name = f"ref{dim}d_{'g_' if gravity else ''}ctw{int(bool(ctw))}"
     return os.path.join(REF_DIR, name)
@@ -67,7 +67,8 @@ def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nth
                     mode, nsteps, prob.flg, nthreads, prob.nout, 0 if phi is None else 1,
                     prob.gam, prob.cfl, prob.dtrec, dt,
                     prob.xmin, prob.xmax, prob.ymin, prob.ymax, prob.zmin, prob.zmax,
-                    prob.nu0, prob.eta0,
+                    # the Hall build reads (di, de) from the (nu0, eta0) fields
+                    *((prob.di, prob.de) if getattr(prob, "hall", False) else (prob.nu0, prob.eta0)),
                     *[int(v) for v in prob.dnx], *[int(v) for v in prob.dny], *[int(v) for v in prob.dnz])
     with open(path, "wb") as f:
         f.write(hdr)
@@ -99,7 +100,7 @@ def read_result(path: str, prob):
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
                   state: Optional[np.ndarray] = None, timeout: float = 3600.0):
     """Run the reference's own code on ``prob`` and return its result dict."""
-    exe = ref_binary(prob.dim, prob.ctw, _phi(prob) is not None)
+    exe = ref_binary(prob.dim, prob.ctw, "hall" if getattr(prob, "hall", False) else _phi(prob) is not None)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"reference oracle binary missing: {exe} (build with `make -C oracle ref`)")
     with tempfile.TemporaryDirectory(prefix="qasref_") as td:
@@ -226,6 +227,10 @@ class Restatement:
                                       ctypes.c_double, ctypes.c_double]
         self.lib.qo_dsptv.restype = ctypes.c_int
         self.lib.qo_kat.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
+        self.lib.qo_hall.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        self.lib.qo_hall.restype = ctypes.c_int
+        self.lib.qo_haldt.argtypes = [ctypes.POINTER(_OGrid), dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        self.lib.qo_haldt.restype = ctypes.c_double
         self.lib.qo_kat.restype = ctypes.c_int
 
     @staticmethod
@@ -272,6 +277,15 @@ class Restatement:
             rc = self.lib.qo_step(ctypes.byref(g), p, dt)
             assert rc == 0
             return {"state": st, "dts": np.array([dt]), "steps": 1, "tim": dt, "dt": dt}
+        hall = getattr(prob, "hall", False)
+        if hall:
+            from qasmhd_b200.problems import hall_vphix
+            vphix = hall_vphix(prob)
+        if mode == MODE_DSTEP and hall:  # the Hall build's DSTEP: bound; one hall_(dt)
+            self.lib.qo_bound(ctypes.byref(g), p)
+            rc = self.lib.qo_hall(ctypes.byref(g), p, dt, prob.di, vphix)
+            assert rc == 0
+            return {"state": st, "dts": np.array([dt]), "steps": 1, "tim": dt, "dt": dt}
         if mode == MODE_DSTEP:
             self.lib.qo_bound(ctypes.byref(g), p)
             rc = self.lib.qo_dsptv(ctypes.byref(g), p, dt, prob.nu0, prob.eta0)
@@ -294,6 +308,11 @@ class Restatement:
             tim += dt
             dts.append(dt)
             self.lib.qo_bound(ctypes.byref(g), p)
+            if hall and prob.di != 0:  # Hall sub-cycles of HMHD1D::exec_ (hmhd1d_class.cpp:26-33)
+                hmax = 1 + int(dt / self.lib.qo_haldt(ctypes.byref(g), p, prob.cfl, prob.di, vphix))
+                for _ in range(hmax):
+                    assert self.lib.qo_hall(ctypes.byref(g), p, dt / hmax, prob.di, vphix) == 0
+                    self.lib.qo_bound(ctypes.byref(g), p)
             rc = self.lib.qo_step(ctypes.byref(g), p, dt)
             assert rc == 0
             if mode == MODE_DRUN:

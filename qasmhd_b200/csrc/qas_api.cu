@@ -21,6 +21,7 @@
 #include "qas_dissip.cuh"
 #include "qas_kernels.cuh"
 #include "qas_tma.cuh"
+#include "qas_hall.cuh"
 
 using namespace qas;
 
@@ -98,6 +99,10 @@ struct qas_ctx {
   // and persistent grid size; lr_tma_ok = supported by this grid, lr_tma = in use
   bool lr_tma_ok = false, lr_tma = false;
   double *d_phi = nullptr;  // gravitational potential of the gravity drivers (qas_set_gravity)
+  // Hall driver (qas_set_hall): ion inertia length, whistler speed factor, haldt reduction
+  bool hall = false;
+  double hall_di = 0.0, hall_vphix = 0.0;
+  unsigned long long *d_hvmax = nullptr, *h_hvmax = nullptr;
   LrTmaMaps lr_maps[3];
   LrTmaPlan lr_plan[3];
   int lr_grid[3] = {0, 0, 0};
@@ -172,7 +177,8 @@ bool build_axis(AxisMap &m, int dim, int n, int st, int dn, int group_dn)
 
 // One (group, field, axis) map.  Groups: 0 the state (bound(val)), 1 cell-centre B
 // (bound(cx,cy,cz) with bx/by/bz's flags, unstaggered: mhd2d_solve.cpp:75-79), 2 the shock
-// detector dv (normal component's flag sign-flipped: mhd2d_solve.cpp:119-125).
+// detector dv (normal component's flag sign-flipped: mhd2d_solve.cpp:119-125), 3 the Hall
+// velocity (the momentum flags, 1D/SERIAL/h-shock/hmhd1d_solve.cpp:185-188).
 static bool map_for(int dim, const qas_bc &bc, int G, int f, int a, int n, AxisMap &m)
 {
   if (a >= dim) return true;
@@ -187,10 +193,14 @@ static bool map_for(int dim, const qas_bc &bc, int G, int f, int a, int n, AxisM
     fdn = dn[a][4 + f];
     gdn = dn[a][4];
     st = 0;
-  } else {
+  } else if (G == 2) {
     auto dvflag = [&](int comp) { return comp == a ? -dn[a][1 + comp] : dn[a][1 + comp]; };
     fdn = dvflag(f);
     gdn = dvflag(0);
+    st = 0;
+  } else {  // G == 3: Hall velocity with the momentum flags, bound(pv,3,&dnxs[1]) (hmhd1d_solve.cpp:185-188)
+    fdn = dn[a][1 + f];
+    gdn = dn[a][1];
     st = 0;
   }
   return build_axis(m, dim, n, st, fdn, gdn);
@@ -200,9 +210,15 @@ static qas_status build_maps(qas_ctx *c)
 {
   const int dim = c->grid.dim;
   const int nmax = std::max(c->geo.nx, std::max(c->geo.ny, c->geo.nz));
-  std::vector<int> src((size_t)3 * 8 * 3 * nmax, 0);
-  std::vector<double> fac((size_t)3 * 8 * 3 * nmax, 1.0);
-  for (int G = 0; G < 3; G++) {
+  std::vector<int> src((size_t)4 * 8 * 3 * nmax, 0);
+  std::vector<double> fac((size_t)4 * 8 * 3 * nmax, 1.0);
+  for (int G = 0; G < 4; G++) {
+    if (G == 3 && dim != 1) {  // the Hall driver is 1D; identity maps elsewhere
+      for (int f = 0; f < 3; f++)
+        for (int a = 0; a < 3; a++)
+          for (int i = 0; i < nmax; i++) src[(size_t)((G * 8 + f) * 3 + a) * nmax + i] = i;
+      continue;
+    }
     const int nf = G == 0 ? 8 : 3;
     for (int f = 0; f < nf; f++) {
       for (int a = 0; a < 3; a++) {
@@ -610,11 +626,71 @@ long long launch_setdt(qas_ctx *c, double cfl, int rule, double dtrec, int nout)
 }
 
 // one exec_ iteration
+// one hall_(dt) call (1D/SERIAL/h-shock/hmhd1d_solve.cpp:138-264): ut = u, R_K stages
+long long launch_hall(qas_ctx *c, double dt)
+{
+  const Geo &g = c->geo;
+  const size_t bytes = (size_t)g.nd * sizeof(double);
+  for (int m = 0; m < 8; m++) cudaMemcpyAsync(c->view.u0[m], c->view.u[m], bytes, cudaMemcpyDeviceToDevice, c->stream);
+  const double dtdx = dt / c->grid.dx, idx = 1.0 / c->grid.dx;
+  const unsigned nb = (unsigned)((g.nx + BLK - 1) / BLK);
+  long long nk = 0;
+  for (int rk = 0; rk < c->scheme.rk; rk++) {
+    double c0, c1;
+    rk_factors(c->scheme.rk, rk, c0, c1);
+    k_hvel<<<nb, BLK, 0, c->stream>>>(c->view, c->hall_di, idx);
+    switch (c->scheme.odr) {
+      case 1: k_hlr<1><<<nb, BLK, 0, c->stream>>>(c->view); break;
+      case 2: k_hlr<2><<<nb, BLK, 0, c->stream>>>(c->view); break;
+      case 3: k_hlr<3><<<nb, BLK, 0, c->stream>>>(c->view); break;
+      default: k_hlr<4><<<nb, BLK, 0, c->stream>>>(c->view); break;
+    }
+    k_hflux<<<nb, BLK, 0, c->stream>>>(c->view, c->hall_vphix);
+    switch (c->scheme.odr) {
+      case 1: k_hupdate<1><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
+      case 2: k_hupdate<2><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
+      case 3: k_hupdate<3><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
+      default: k_hupdate<4><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
+    }
+    k_bound<<<shell_grid(g), BLK, 0, c->stream>>>(c->view);
+    nk += 5;
+  }
+  return nk;
+}
+
+// the Hall sub-cycles of HMHD1D::exec_ (1D/SERIAL/h-shock/hmhd1d_class.cpp:26-33): hmax =
+// 1 + (int)(dt/haldt()) with haldt = cfl*dx/max(1, max |hx| + vphix |bx/ro|), read back to the
+// host (1D grids are small; this is one short synchronisation per step)
+long long launch_hall_subcycles(qas_ctx *c, double cfl)
+{
+  static const double one = 1.0;
+  cudaMemcpyAsync(c->d_hvmax, &one, sizeof(one), cudaMemcpyHostToDevice, c->stream);
+  const unsigned nb = (unsigned)((c->geo.nx - 2 * GH + BLK - 1) / BLK);
+  k_hall_vmax<<<nb, BLK, 0, c->stream>>>(c->view, c->hall_vphix, c->d_hvmax);
+  cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(c->h_hvmax, c->d_hvmax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess || c->h_ctl->done) return 1;
+  const double dt = c->h_ctl->dt;
+  const double vmax = __builtin_bit_cast(double, *c->h_hvmax);
+  const double haldt = cfl * c->grid.dx / vmax;
+  const int hmax = 1 + (int)(dt / haldt);
+  long long nk = 1;
+  for (int h = 0; h < hmax; h++) {
+    nk += launch_hall(c, dt / hmax);
+    k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view);
+    nk++;
+  }
+  return nk;
+}
+
+bool hall_active(const qas_ctx *c) { return c->hall && c->hall_di != 0; }
+
 long long launch_exec_step(qas_ctx *c, const qas_run_opts &o, int n_after)
 {
   long long nk = 0;
   QL(c, KID_BEGIN, k_begin_step<<<1, 1, 0, c->stream>>>(c->view, o.stop_rule == 2 ? 0 : 1));
   QL(c, KID_BOUND, k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view));
+  if (hall_active(c)) nk += launch_hall_subcycles(c, o.cfl);
   nk += 2 + launch_ideal(c);
   if (c->grid.dim >= 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
   if (o.flg && (n_after % 2 == 0)) nk += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
@@ -801,6 +877,8 @@ qas_status qas_destroy(qas_ctx *c)
   if (c->d_dctl) cudaFree(c->d_dctl);
   if (c->d_scratch) cudaFree(c->d_scratch);
   if (c->d_phi) cudaFree(c->d_phi);
+  if (c->d_hvmax) cudaFree(c->d_hvmax);
+  if (c->h_hvmax) cudaFreeHost(c->h_hvmax);
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -957,7 +1035,7 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
     n_host++;
     launched++;
   }
-  const bool want_graph = o.use_graph != 0;
+  const bool want_graph = o.use_graph != 0 && !hall_active(c);  // the Hall sub-cycle count is read back
   if (want_graph && launched + 2 <= limit) {
     const bool stale = !c->graph || c->graph_flg != o.flg || c->graph_rule != o.stop_rule || c->graph_cfl != o.cfl ||
                        c->graph_nu0 != o.nu0 || c->graph_eta0 != o.eta0 || c->graph_dtrec != o.dtrec ||
@@ -1102,7 +1180,7 @@ qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int fie
                       double *fac, int n)
 {
   if (!grid || !bc || !src || !fac) return QAS_ERR_INVALID;
-  if (group < 0 || group > 2 || field < 0 || field >= (group == 0 ? 8 : 3) || axis < 0 || axis > 2)
+  if (group < 0 || group > 3 || field < 0 || field >= (group == 0 ? 8 : 3) || axis < 0 || axis > 2)
     return QAS_ERR_INVALID;
   const int ext[3] = {grid->nxm + 2 * GH, grid->dim >= 2 ? grid->nym + 2 * GH : 1,
                       grid->dim >= 3 ? grid->nzm + 2 * GH : 1};
@@ -1170,6 +1248,41 @@ qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas
   }
   *count = w;
   return read_ctl(c);
+}
+
+qas_status qas_set_hall(qas_ctx *c, double di, double de)
+{
+  if (!c || !(di >= 0.0) || !(de >= 0.0)) return QAS_ERR_INVALID;
+  if (c->grid.dim != 1 || de != 0.0) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if (!c->d_hvmax && cudaMalloc(&c->d_hvmax, sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return QAS_ERR_NOMEM;
+  }
+  if (!c->h_hvmax && cudaMallocHost(&c->h_hvmax, sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return QAS_ERR_NOMEM;
+  }
+  // HMHD1D::paras (1D/SERIAL/h-shock/hmhd1d_paras.cpp:29-34) with de = 0
+  const double idx = 1.0 / c->grid.dx;
+  const double kpeak = M_PI * idx;
+  c->hall = true;
+  c->hall_di = di;
+  c->hall_vphix = di * kpeak;
+  return QAS_OK;
+}
+
+qas_status qas_hall(qas_ctx *c, double dt)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (!c->hall) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
+  c->launches += launch_hall(c, dt);
+  return check_launch(c);
 }
 
 qas_status qas_set_gravity(qas_ctx *c, const double *phi_g)

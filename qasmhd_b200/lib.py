@@ -39,6 +39,7 @@ EXPORTS = (
     "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
     "qas_bkup_load", "qas_dd_plan", "qas_dd_create", "qas_dd_destroy", "qas_dd_upload_block",
     "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches", "qas_set_gravity",
+    "qas_set_hall", "qas_hall",
 )
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
@@ -167,6 +168,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                   ctypes.POINTER(BC), ctypes.c_int, ip]
     lib.qas_dd_destroy.argtypes = [vp]
     lib.qas_set_gravity.argtypes = [vp, dp]
+    lib.qas_set_hall.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    lib.qas_hall.argtypes = [vp, ctypes.c_double]
     lib.qas_dd_upload_block.argtypes = [vp, dp]
     lib.qas_dd_download_block.argtypes = [vp, dp]
     lib.qas_dd_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
@@ -221,7 +224,17 @@ class Context:
                   prob.dnx, prob.dny, prob.dnz, device)
         if getattr(prob, "phi", None) is not None:
             ctx.set_gravity(prob.phi)
+        if getattr(prob, "hall", False):
+            ctx.set_hall(prob.di, prob.de)
         return ctx
+
+    def set_hall(self, di: float, de: float = 0.0) -> None:
+        """qas_set_hall: the Hall form of the 1D driver (ion / electron inertia lengths)."""
+        _check(self.lib.qas_set_hall(self.h, float(di), float(de)), "qas_set_hall")
+
+    def hall(self, dt: float) -> None:
+        """qas_hall: one hall_(dt) call."""
+        _check(self.lib.qas_hall(self.h, float(dt)), "qas_hall")
 
     def set_gravity(self, phi: Optional[np.ndarray]) -> None:
         """qas_set_gravity: the gravitational potential of every padded cell, or None (off)."""

@@ -62,6 +62,11 @@ class Problem:
     state: Optional[np.ndarray] = None  # shape (8, nz, ny, nx) incl. ghosts
     # gravitational potential phi_g (nz, ny, nx) of the gravity drivers, None without gravity
     phi: Optional[np.ndarray] = None
+    # Hall driver (1D/SERIAL/h-shock, HMHD1D): on/off, ion inertia length di, electron inertia
+    # length de (absolute, = dx*D_ELE)
+    hall: bool = False
+    di: float = 0.0
+    de: float = 0.0
 
     @property
     def nx(self) -> int:
@@ -169,6 +174,36 @@ def brio_wu(nxm: int = 1024, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3,
     st = _pack(ro, z, z, z, bx, by, z, pr, bx, by, z, p.gam)
     p.state = st.reshape(NM, 1, 1, p.nx)
     return p
+
+
+def hall_shock(nxm: int = 400, di: float = 1e-3, rmn: int = RMN_LHLLD, odr: int = 4, rk: int = 3,
+               tmax: float = 1.0, nout: int = 1) -> Problem:
+    """Brio-Wu states of the Hall driver (1D/SERIAL/h-shock/mhd1d_init_.cpp, NUM 2) on
+    x in [-0.5, 0.5] split at x <= 0, gamma = 2, Neumann (+1) boundaries for every field
+    (hmhd1d_paras.cpp:6-20), ion inertia length di, no electron inertia (D_ELE = 0), and the
+    driver's exec_(0) loop (constant dt, h-shock/main.cpp)."""
+    p = Problem(name=f"hallshock_{nxm}", dim=1, nxm=nxm, rmn=rmn, odr=odr, rk=rk, ctw=0, gam=2.0, cfl=0.4,
+                dtrec=tmax, nout=nout, xmin=-0.5, xmax=0.5, dnx=(1,) * NM, flg=0, hall=True, di=di, de=0.0)
+    x, _, _ = p.coords()
+    left = x <= 0
+    ro = np.where(left, 1.0, 0.125)
+    pr = np.where(left, 1.0, 0.1)
+    z = np.zeros_like(x)
+    bx = np.full_like(x, 0.75)
+    by = np.where(left, 1.0, -1.0)
+    st = _pack(ro, z, z, z, bx, by, z, pr, bx, by, z, p.gam)
+    p.state = st.reshape(NM, 1, 1, p.nx)
+    return p
+
+
+def hall_vphix(prob) -> float:
+    """Whistler speed factor of HMHD1D::paras (1D/SERIAL/h-shock/hmhd1d_paras.cpp:29-34)."""
+    idx = 1.0 / prob.dx
+    kpeak = math.pi * idx
+    if prob.de != 0:
+        k_e = 1.0 / prob.de
+        kpeak = k_e if kpeak >= k_e else kpeak  # min() of common/common_func.h
+    return prob.di * kpeak
 
 
 # ----------------------------------------------------------------------------

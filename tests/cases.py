@@ -21,7 +21,10 @@ def run_gpu(prob, mode: int, nsteps: int = 0, dt: float = 0.0, use_graph: bool =
             return {"state": out, "steps": 1}
         if mode == R.MODE_DSTEP:
             ctx.bound()
-            ctx.dsptv(dt, prob.nu0, prob.eta0)
+            if getattr(prob, "hall", False):  # the Hall build's DSTEP: one hall_(dt)
+                ctx.hall(dt)
+            else:
+                ctx.dsptv(dt, prob.nu0, prob.eta0)
             out = ctx.download(st.shape)
             ctx.sync()
             return {"state": out, "steps": 1}

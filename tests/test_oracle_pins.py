@@ -96,3 +96,17 @@ def test_live_reference_gravity(restatement, dim, ctw, rmn):
     a = R.run_reference(p, R.MODE_STEP, dt=1e-3, nthreads=2)
     b = restatement.run(p, 1, mode=R.MODE_STEP, dt=1e-3)
     assert_bitwise(b["state"], a["state"], f"rt{dim}d step")
+
+
+@pytest.mark.skipif(not R.reference_available(1, 0, gravity="hall"), reason="reference Hall build not built")
+@pytest.mark.parametrize("di,odr", [(1e-3, 4), (0.05, 4), (0.02, 2)])
+def test_live_reference_hall(restatement, di, odr):
+    """The 1D Hall driver (1D/SERIAL/h-shock, HMHD1D): one hall_ call, and runs with the Hall
+    sub-cycles of exec_ (di = 0.05 gives tens of sub-cycles per step)."""
+    p = P.hall_shock(64, di=di, odr=odr, rk=3 if odr == 4 else 2)
+    a = R.run_reference(p, R.MODE_DSTEP, dt=1e-3, nthreads=1)
+    b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=1e-3)
+    assert_bitwise(b["state"], a["state"], "hall_")
+    a = R.run_reference(p, R.MODE_RUN, nsteps=4, nthreads=1)
+    b = restatement.run(p, 4, mode=R.MODE_RUN)
+    assert_bitwise(b["state"], a["state"], "hall run")
