@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "bw1d_1024"], default="ot2d_1024")
+    ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "kh3d_128", "bw1d_1024"], default="ot2d_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lr-staging", type=int, choices=[0, 1], default=None,
                     help="reconstruction stencils: 1 = TMA-staged in shared memory, 0 = global loads "
@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-decomposed", action="store_true",
+                    help="skip the slab-decomposition leg (KH 256^3 in 4 z-slabs on this GPU vs one domain)")
     ap.add_argument("--no-plain3d", action="store_true",
                     help="skip the 3D Kelvin-Helmholtz 256^3 leg (GPU vs the reference's OpenMP build)")
     ap.add_argument("--adjoint-only", action="store_true",
@@ -89,6 +91,10 @@ def make_problem(name):
         p = P.orszag_tang(1024)
         cfg = {"workload": "orszag_tang_2d_1024x1024", "grid": [1024, 1024], "solver": "HLLD", "order": "WCNS4",
                "rk": 3, "ct": "CUCT", "bc": "periodic", "gamma": "5/3"}
+    elif name == "kh3d_128":  # a smaller case of the same workload, for profiler captures
+        p = P.kelvin_helmholtz(3, 128)
+        cfg = {"workload": "kelvin_helmholtz_3d_128^3", "grid": [128, 128, 128], "solver": "MLAU",
+               "order": "WCNS4", "rk": 3, "ct": "CUCT", "bc": "periodic x,z / open y", "mach": 0.01, "beta": 100}
     elif name == "kh3d_256":
         p = P.kelvin_helmholtz(3, 256)
         cfg = {"workload": "kelvin_helmholtz_3d_256^3", "grid": [256, 256, 256], "solver": "MLAU",
@@ -251,6 +257,41 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
                              "unit": "GB/s", "basis": "512 algorithmic B per cell-update"}}
     if cpu:
         out["ratio_vs_cpu"] = gpu / cpu["value"]
+    return out
+
+
+def decomposed_compare(nparts=4, steps=6):
+    """KH 256^3 split into z-slabs (qas_dd_*: ghost-plane copies after each fill, primitive pass
+    and shock detector; gathered CFL maximum) on this one GPU, against the single domain, both
+    eager (no graph), wall time around the run call with a device synchronise on both sides:
+    the cost of the exchanges themselves, which on several GPUs become NVLink peer copies."""
+    import torch
+
+    from qasmhd_b200 import lib as L
+    from qasmhd_b200 import problems as P
+    prob = P.kelvin_helmholtz(3, 256)
+    out = {"workload": "kelvin_helmholtz_3d_256^3", "nparts": nparts, "steps": steps, "timing": "host wall, synced"}
+    with L.Context.from_problem(prob) as ctx:
+        ctx.upload(prob.state)
+        ctx.run(max_steps=2, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.run(max_steps=steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=False)
+        torch.cuda.synchronize()
+        single = (time.perf_counter() - t0) / steps
+    with L.Decomposition(prob, nparts) as dd:
+        dd.upload(prob.state)
+        dd.run(max_steps=2, flg=1, stop_rule=0, cfl=prob.cfl)
+        torch.cuda.synchronize()
+        k0, c0 = dd.kernel_launches()
+        t0 = time.perf_counter()
+        dd.run(max_steps=steps, flg=1, stop_rule=0, cfl=prob.cfl)
+        torch.cuda.synchronize()
+        split = (time.perf_counter() - t0) / steps
+        k1, c1 = dd.kernel_launches()
+    out.update({"single_ms_per_step": 1e3 * single, "split_ms_per_step": 1e3 * split,
+                "overhead": split / single - 1.0, "copies_per_step": (c1 - c0) / steps,
+                "split_mcells": prob.interior_cells / split / 1e6})
     return out
 
 
@@ -467,6 +508,9 @@ def main():
     if rank == 0 and not args.no_adjoint and world == 1:
         ctx.close()
         line["adjoint"] = adjoint_compare()
+    if rank == 0 and not args.no_decomposed and world == 1:
+        ctx.close()
+        line["decomposed"] = decomposed_compare()
     if rank == 0 and not args.no_plain3d and world == 1 and args.workload != "kh3d_256":
         ctx.close()
         line["plain3d"] = plain3d_compare(cpu_steps=0 if args.no_cpu_baseline else 2)

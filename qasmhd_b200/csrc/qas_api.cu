@@ -442,9 +442,16 @@ void launch_lr(qas_ctx *c, int a)
 template <int RMN>
 void launch_flux(qas_ctx *c, int a)
 {
-  if (a == 0) QL(c, KID_FLUX, k_flux<RMN, 0><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
-  if (a == 1) QL(c, KID_FLUX, k_flux<RMN, 1><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
-  if (a == 2) QL(c, KID_FLUX, k_flux<RMN, 2><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+  if constexpr (RMN == 3) {
+    if (a == 0) QL(c, KID_FLUX, k_flux_mlau<0><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+    if (a == 1) QL(c, KID_FLUX, k_flux_mlau<1><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+    if (a == 2) QL(c, KID_FLUX, k_flux_mlau<2><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+    return;
+  } else {
+    if (a == 0) QL(c, KID_FLUX, k_flux<RMN, 0><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+    if (a == 1) QL(c, KID_FLUX, k_flux<RMN, 1><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+    if (a == 2) QL(c, KID_FLUX, k_flux<RMN, 2><<<cells_grid(c->geo, c->tile[KID_FLUX]), c->tile[KID_FLUX], 0, c->stream>>>(c->view));
+  }
 }
 
 template <int ODR, int RMN>

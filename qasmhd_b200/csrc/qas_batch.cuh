@@ -68,6 +68,18 @@ __global__ void __launch_bounds__(128) kb_flux(const View *__restrict__ views, B
   QAS_BATCH_END
 }
 
+// MLAU with the register cap of the single-grid k_flux_mlau
+template <int A>
+__global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kb_flux_mlau(const View *__restrict__ views, BMap map)
+{
+  QAS_BATCH_BLOCKS(map)
+  if (QAS_BATCH_CELL_OK) {
+    const int pos = A == 0 ? ti : (A == 1 ? tj : tk);
+    if (pos >= 3 && pos < v.g.n[A] - 2) flux_body<3, A>(v, ti, tj, tk);
+  }
+  QAS_BATCH_END
+}
+
 template <int ODR>
 __global__ void kb_emf(const View *__restrict__ views, BMap map)
 {
