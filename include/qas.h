@@ -186,8 +186,10 @@ qas_status qas_profile_run(qas_ctx *ctx, const qas_run_opts *opts, int nsteps, q
  * hmax = 1 + (int)(dt/haldt) Hall sub-cycles hall_(dt/hmax), each followed by bound(),
  * between the ghost fill and ideal(dt) (hmhd1d_class.cpp:15-44; haldt: :3-13), with
  * vphix = di*pi/dx (hmhd1d_paras.cpp:29-34).  The sub-cycle count is read back each step, so
- * qas_run runs such a context without graph capture.  QAS_ERR_UNSUPPORTED for dim != 1 and for
- * de != 0 (the electron-inertia correction solve, hmhd1d_solve.cpp:266-426, is not built).
+ * qas_run runs such a context without graph capture.  With de != 0 the by/bz fluxes of ideal()
+ * and hall_() get the electron-inertia correction crcte: a conjugate-gradient solve of
+ * (1 - de^2 d2/dx2) E = E_flux per flux (hmhd1d_solve.cpp:266-426), run in one CTA with the
+ * reference's summation order.  QAS_ERR_UNSUPPORTED for dim != 1.
  * qas_hall: one hall_(dt) call (no ghost fill before), QAS_ERR_UNSUPPORTED without the Hall form. */
 qas_status qas_set_hall(qas_ctx *ctx, double di, double de);
 qas_status qas_hall(qas_ctx *ctx, double dt);

@@ -1224,6 +1224,75 @@ static inline double d4(const double *p, long ss, long s, pt_fn df)
   return df(&f[1]);
 }
 
+/* bc1d (common/common_func.c:34-58) of one array with any flag value (flags outside
+ * {0, +-1, +-2} leave the ghosts alone) */
+static void bc1d_any(double *f, int nx, int dn)
+{
+  int i;
+  if (dn == 0) {
+    for (i = 0; i < GH; i++) { f[i] = f[nx - 2 * GH + i]; f[nx - 1 - i] = f[2 * GH - 1 - i]; }
+  } else if (abs(dn) == 1) {
+    for (i = 0; i < GH; i++) { f[i] = dn * f[2 * GH - 1 - i]; f[nx - 1 - i] = dn * f[nx - 2 * GH + i]; }
+  } else if (abs(dn) == 2) {
+    for (i = 0; i < GH; i++) { f[i] = 0.25 * (2 + dn) * f[GH]; f[nx - 1 - i] = 0.25 * (2 + dn) * f[nx - 1 - GH]; }
+  }
+}
+
+static double d2f2(const double *f) { return ((f[1] + f[-1]) - 2.0 * f[0]); }
+static double d2f4(const double *f) { return ((-(f[2] + f[-2]) + 16.0 * (f[1] + f[-1]) - 30.0 * f[0]) / 12.0); }
+
+/* HMHD1D::crcte (1D/SERIAL/h-shock/hmhd1d_solve.cpp:275-300) with eorg2enew_cg (:326-403):
+ * fbt/fen = the by (or bz) and energy fluxes (stride 1 here), bt = by (or bz), dn = the flag
+ * product; the density passed to the solve is 1 everywhere, as crcte does.  Faces 0..2 and
+ * nx-2.. are never read by the update, so their (reference: uninitialised) inputs do not matter. */
+static void crcte(double *fbt, double *fen, const double *bt, int nx, int dn, double de, double dx, int odr)
+{
+  int i;
+  double *eorg = xcalloc(nx), *enew = xcalloc(nx), *rk = xcalloc(nx), *pk = xcalloc(nx), *ap = xcalloc(nx);
+  const double one = 1.0;
+  pt_fn d2f = odr >= 3 ? d2f4 : d2f2;
+  for (i = 0; i < nx; i++) eorg[i] = enew[i] = fbt[i];
+  const int cmax = nx;
+  const double eps = 1e-8, fac = (de * de) / (dx * dx);
+  int cnt = 0;
+  double numer = 0.0, denom, coef, anorm, anormf = 0.0;
+  bc1d_any(enew, nx, dn);
+  for (i = GH; i < nx - GH; i++) {
+    rk[i] = one * eorg[i] - (one * enew[i] - fac * d2f(&enew[i]));
+    pk[i] = rk[i];
+    numer += rk[i] * rk[i];
+    anormf += fabs(rk[i]);
+  }
+  do {
+    bc1d_any(pk, nx, dn);
+    denom = 0.0;
+    for (i = GH; i < nx - GH; i++) {
+      ap[i] = (one * pk[i] - fac * d2f(&pk[i]));
+      denom += pk[i] * ap[i];
+    }
+    coef = (denom == 0) ? 0 : numer / denom;
+    anorm = 0.0;
+    for (i = GH; i < nx - GH; i++) {
+      enew[i] += coef * pk[i];
+      rk[i] -= coef * ap[i];
+      anorm += fabs(rk[i]);
+    }
+    denom = numer;
+    numer = 0.0;
+    for (i = GH; i < nx - GH; i++) numer += rk[i] * rk[i];
+    coef = (denom == 0) ? 0 : numer / denom;
+    for (i = GH; i < nx - GH; i++) pk[i] = rk[i] + coef * pk[i];
+  } while ((anorm > eps * anormf) && (++cnt < cmax));
+  bc1d_any(enew, nx, dn);
+  for (i = 1; i < nx; i++) {
+    double dd = enew[i] - eorg[i];
+    double bb = 0.5 * (bt[i - 1] + bt[i]);
+    fbt[i] = enew[i];
+    fen[i] += dd * bb;
+  }
+  free(eorg); free(enew); free(rk); free(pk); free(ap);
+}
+
 static void ideal_stage(const geo *e, double *const *u, work *w, int rk, double dt)
 {
   const qo_grid *g = e->g;
@@ -1312,6 +1381,12 @@ static void ideal_stage(const geo *e, double *const *u, work *w, int rk, double 
   /* face sweeps */
   for (int a = 0; a < dim; a++) sweep(e, (const double *const *)u, w, a);
   if (dim >= 2) corner_emfs(e, w);
+  if (dim == 1 && g->hall_de != 0) {
+    /* HMHD1D::ideal's electron-inertia correction (1D/SERIAL/h-shock/hmhd1d_solve.cpp:98-108) */
+    double *F = w->flx[0];
+    crcte(F + 5 * nd, F + 7 * nd, u[5], nx, g->dnx[1] * g->dnx[5], g->hall_de, g->dx, g->odr);
+    crcte(F + 6 * nd, F + 7 * nd, u[6], nx, g->dnx[1] * g->dnx[6], g->hall_de, g->dx, g->odr);
+  }
 
   /* centre update: mhd2d_solve.cpp:341-358, mhd3d_solve.cpp:658-676, mhd1d_solve.cpp:97-113 */
   int cen1[7] = {0, 1, 2, 3, 5, 6, 7};
@@ -1850,6 +1925,10 @@ int qo_hall(const qo_grid *g, double *u, double dt, double di, double vphix)
       smax += qmax(fabs(L[1]), fabs(R[1]));
       smax += vphix * fabs(bn / rn);
       flux_hall_lf(L, R, bn, smax, &fx[i], &fx[nx + i], &fx[2 * nx + i]);
+    }
+    if (g->hall_de != 0) {  /* hmhd1d_solve.cpp:232-240 */
+      crcte(fx, fx + 2 * nx, f[5], nx, g->dnx[1] * g->dnx[5], g->hall_de, g->dx, g->odr);
+      crcte(fx + nx, fx + 2 * nx, f[6], nx, g->dnx[1] * g->dnx[6], g->hall_de, g->dx, g->odr);
     }
     /* update of by, bz, en (mhd_updt1d) */
     for (i = GH; i < nx - GH; i++) {

@@ -27,6 +27,8 @@ typedef struct {
   int dnx[8], dny[8], dnz[8];   /* boundary flags per field */
   const double *phi;   /* gravitational potential phi_g (nd doubles), NULL without gravity:
                           the gravity form of the 2D/3D drivers (2D/SERIAL/RTI, 3D/MPI/RTI) */
+  double hall_de;      /* 1D Hall driver's electron inertia length de (absolute); when non-zero
+                          the by/bz fluxes of ideal() and hall_() get the crcte correction */
 } qo_grid;
 
 /* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,
@@ -54,7 +56,9 @@ int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0
 /* Hall term of the 1D Hall driver (1D/SERIAL/h-shock): one hall_(dt) call
  * (hmhd1d_solve.cpp:138-264) with ion inertia length di and whistler speed factor vphix and
  * no electron inertia (de = 0), and haldt() (hmhd1d_class.cpp:3-13), which returns the
- * Hall sub-cycle time step cfl*dx/max(1, max_i |hx| + vphix |bx/ro|). */
+ * Hall sub-cycle time step cfl*dx/max(1, max_i |hx| + vphix |bx/ro|).  With g->hall_de != 0
+ * both hall_ and the 1D ideal step apply the electron-inertia correction (crcte with a CG
+ * solve, hmhd1d_solve.cpp:266-426). */
 int qo_hall(const qo_grid *g, double *u, double dt, double di, double vphix);
 double qo_haldt(const qo_grid *g, const double *u, double cfl, double di, double vphix);
 

@@ -203,7 +203,7 @@ class _OGrid(ctypes.Structure):
                 ("gam", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double),
                 ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8),
-                ("phi", ctypes.POINTER(ctypes.c_double))]
+                ("phi", ctypes.POINTER(ctypes.c_double)), ("hall_de", ctypes.c_double)]
 
 
 class Restatement:
@@ -243,6 +243,8 @@ class Restatement:
         g.dz = prob.dz if prob.dim >= 3 else 0.0
         for m in range(8):
             g.dnx[m], g.dny[m], g.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+        if getattr(prob, "hall", False):
+            g.hall_de = float(prob.de)
         phi = _phi(prob)
         if phi is not None:
             g._phi_keep = phi  # the pointer below must outlive the call

@@ -101,7 +101,7 @@ struct qas_ctx {
   double *d_phi = nullptr;  // gravitational potential of the gravity drivers (qas_set_gravity)
   // Hall driver (qas_set_hall): ion inertia length, whistler speed factor, haldt reduction
   bool hall = false;
-  double hall_di = 0.0, hall_vphix = 0.0;
+  double hall_di = 0.0, hall_vphix = 0.0, hall_de = 0.0;
   unsigned long long *d_hvmax = nullptr, *h_hvmax = nullptr;
   LrTmaMaps lr_maps[3];
   LrTmaPlan lr_plan[3];
@@ -470,6 +470,36 @@ void launch_sweep(qas_ctx *c, int a)
   }
 }
 
+// HMHD1D::crcte on the by and bz fluxes (1D Hall driver with electron inertia), after the
+// flux and before the update of ideal() and hall_(); scratch = the face-state arrays, which
+// the stage no longer needs at that point
+long long launch_crcte(qas_ctx *c)
+{
+  if (!(c->hall && c->hall_de != 0 && c->geo.dim == 1)) return 0;
+  View &v = c->view;
+  const double fac = (c->hall_de * c->hall_de) / (c->grid.dx * c->grid.dx);
+  const int *dn = c->bc.dnx;
+  double *w[5] = {v.vl[0], v.vl[1], v.vl[2], v.vl[3], v.vl[4]};
+  for (int q = 0; q < 2; q++) {
+    double *fbt = v.f[0][5 + q];
+    const double *bt = v.u[5 + q];
+    const int flag = dn[1] * dn[5 + q];
+    switch (c->scheme.odr) {
+#define QAS_CRCTE(O)                                                                                  \
+  case O:                                                                                             \
+    k_crcte<O><<<1, 1024, 0, c->stream>>>(v, fbt, v.f[0][7], bt, flag, fac, w[0], w[1], w[2], w[3], w[4]); \
+    break;
+      QAS_CRCTE(1)
+      QAS_CRCTE(2)
+      QAS_CRCTE(3)
+      default:
+      QAS_CRCTE(4)
+#undef QAS_CRCTE
+    }
+  }
+  return 2;
+}
+
 // one SSP-RK stage in three phases (a domain split into slabs exchanges ghost planes
 // between them): primitives + cell-centre B; the shock detector; sweeps, EMF, update, fill
 template <int ODR>
@@ -510,6 +540,7 @@ long long stage_rest(qas_ctx *c, double c0, double c1)
     }
     nk += 2;
   }
+  nk += launch_crcte(c);  // 1D Hall driver with electron inertia (hmhd1d_solve.cpp:98-108)
   if (g.dim >= 2) {
     QL(c, KID_EMF, k_emf<ODR><<<cells_grid(g, c->tile[KID_EMF]), c->tile[KID_EMF], 0, c->stream>>>(c->view));
     nk++;
@@ -653,6 +684,7 @@ long long launch_hall(qas_ctx *c, double dt)
       default: k_hlr<4><<<nb, BLK, 0, c->stream>>>(c->view); break;
     }
     k_hflux<<<nb, BLK, 0, c->stream>>>(c->view, c->hall_vphix);
+    nk += launch_crcte(c);  // hmhd1d_solve.cpp:232-240
     switch (c->scheme.odr) {
       case 1: k_hupdate<1><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
       case 2: k_hupdate<2><<<nb, BLK, 0, c->stream>>>(c->view, dtdx, c0, c1); break;
@@ -1260,7 +1292,7 @@ qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas
 qas_status qas_set_hall(qas_ctx *c, double di, double de)
 {
   if (!c || !(di >= 0.0) || !(de >= 0.0)) return QAS_ERR_INVALID;
-  if (c->grid.dim != 1 || de != 0.0) return QAS_ERR_UNSUPPORTED;
+  if (c->grid.dim != 1) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   if (c->graph) {
     cudaGraphExecDestroy(c->graph);
@@ -1274,11 +1306,13 @@ qas_status qas_set_hall(qas_ctx *c, double di, double de)
     cudaGetLastError();
     return QAS_ERR_NOMEM;
   }
-  // HMHD1D::paras (1D/SERIAL/h-shock/hmhd1d_paras.cpp:29-34) with de = 0
+  // HMHD1D::paras (1D/SERIAL/h-shock/hmhd1d_paras.cpp:29-34)
   const double idx = 1.0 / c->grid.dx;
-  const double kpeak = M_PI * idx;
+  double kpeak = M_PI * idx;
+  if (de != 0) kpeak = hmin(kpeak, 1.0 / de);
   c->hall = true;
   c->hall_di = di;
+  c->hall_de = de;
   c->hall_vphix = di * kpeak;
   return QAS_OK;
 }

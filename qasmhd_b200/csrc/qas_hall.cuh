@@ -1,6 +1,12 @@
 // qas_hall.cuh -- Hall term of the 1D Hall driver on sm_100a: HMHD1D::hall_
 // (1D/SERIAL/h-shock/hmhd1d_solve.cpp:138-264) and HMHD1D::haldt
-// (1D/SERIAL/h-shock/hmhd1d_class.cpp:3-13), without electron inertia (de = 0).
+// (1D/SERIAL/h-shock/hmhd1d_class.cpp:3-13).
+//
+// With an electron inertia length de != 0, the by/bz fluxes of hall_ and of the 1D ideal
+// step get HMHD1D::crcte (hmhd1d_solve.cpp:275-300): Enew solves (1 - de^2 d2/dx2) Enew = Eorg by
+// the reference's conjugate-gradient loop (eorg2enew_cg, :326-403) in one CTA -- the vector
+// updates in parallel, every sum (numer, denom, anorm, anormf) by one thread in index order, as
+// the reference accumulates them -- so the iterates and the stop test are bit-identical.
 //
 // One hall_(dt) call: ut = u, then per SSP-RK stage
 //   k_hvel     Hall velocity h = -(di/ro) rot B at every cell, its ghosts filled as a gather
@@ -132,6 +138,107 @@ __global__ void k_hupdate(View v, double dtdx, double c0, double c1)
   }
 #pragma unroll
   for (int q = 0; q < 3; q++) v.u[5 + q][i] = nv[q];
+}
+
+// bc1d (common/common_func.c:34-58) of one array with any flag (others leave the ghosts alone);
+// threads 0..GH-1 fill one lower and one upper ghost each, sources are interior cells
+__device__ __forceinline__ void bc1d_any(double *f, int nx, int dn, int t)
+{
+  if (t >= GH) return;
+  if (dn == 0) {
+    f[t] = f[nx - 2 * GH + t];
+    f[nx - 1 - t] = f[2 * GH - 1 - t];
+  } else if (dn == 1 || dn == -1) {
+    f[t] = dn * f[2 * GH - 1 - t];
+    f[nx - 1 - t] = dn * f[nx - 2 * GH + t];
+  } else if (dn == 2 || dn == -2) {
+    f[t] = 0.25 * (2 + dn) * f[GH];
+    f[nx - 1 - t] = 0.25 * (2 + dn) * f[nx - 1 - GH];
+  }
+}
+
+// df2[ODR-1] (common/common_interp.h:27-35)
+template <int ODR>
+__device__ __forceinline__ double d2f(const double *f, int i)
+{
+  if (ODR >= 3) return (-(f[i + 2] + f[i - 2]) + 16.0 * (f[i + 1] + f[i - 1]) - 30.0 * f[i]) / 12.0;
+  return (f[i + 1] + f[i - 1]) - 2.0 * f[i];
+}
+
+// crcte of one flux pair, one CTA: fbt = the by or bz flux, fen = the energy flux, bt = by or bz,
+// dn = the flag product, fac = de^2/dx^2; eorg, enew, rk, pk, ap = scratch arrays of nx doubles
+template <int ODR>
+__global__ void __launch_bounds__(1024) k_crcte(View v, double *fbt, double *fen, const double *bt, int dn,
+                                                double fac, double *eorg, double *enew, double *rk, double *pk,
+                                                double *ap)
+{
+  if (v.ctl->done) return;
+  const int nx = v.g.nx, t = threadIdx.x, nt = blockDim.x;
+  const double one = 1.0, eps = 1e-8;
+  __shared__ double s_numer, s_anormf, s_coef, s_coef2;
+  __shared__ int s_go;
+  for (int i = t; i < nx; i += nt) eorg[i] = enew[i] = fbt[i];
+  __syncthreads();
+  bc1d_any(enew, nx, dn, t);
+  __syncthreads();
+  for (int i = GH + t; i < nx - GH; i += nt) {
+    const double r = one * eorg[i] - (one * enew[i] - fac * d2f<ODR>(enew, i));
+    rk[i] = r;
+    pk[i] = r;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double numer = 0.0, anormf = 0.0;
+    for (int i = GH; i < nx - GH; i++) {
+      numer += rk[i] * rk[i];
+      anormf += fabs(rk[i]);
+    }
+    s_numer = numer;
+    s_anormf = anormf;
+  }
+  __syncthreads();
+  int cnt = 0;  // thread 0's copy decides
+  const int cmax = nx;
+  for (;;) {
+    bc1d_any(pk, nx, dn, t);
+    __syncthreads();
+    for (int i = GH + t; i < nx - GH; i += nt) ap[i] = (one * pk[i] - fac * d2f<ODR>(pk, i));
+    __syncthreads();
+    if (t == 0) {
+      double denom = 0.0;
+      for (int i = GH; i < nx - GH; i++) denom += pk[i] * ap[i];
+      s_coef = (denom == 0) ? 0 : s_numer / denom;
+    }
+    __syncthreads();
+    const double coef = s_coef;
+    for (int i = GH + t; i < nx - GH; i += nt) {
+      enew[i] += coef * pk[i];
+      rk[i] -= coef * ap[i];
+    }
+    __syncthreads();
+    if (t == 0) {
+      double anorm = 0.0, numer = 0.0;
+      for (int i = GH; i < nx - GH; i++) anorm += fabs(rk[i]);
+      const double denom = s_numer;
+      for (int i = GH; i < nx - GH; i++) numer += rk[i] * rk[i];
+      s_numer = numer;
+      s_coef2 = (denom == 0) ? 0 : numer / denom;
+      s_go = (anorm > eps * s_anormf) && (++cnt < cmax);
+    }
+    __syncthreads();
+    const double coef2 = s_coef2;
+    for (int i = GH + t; i < nx - GH; i += nt) pk[i] = rk[i] + coef2 * pk[i];
+    __syncthreads();
+    if (!s_go) break;
+  }
+  bc1d_any(enew, nx, dn, t);
+  __syncthreads();
+  for (int i = 1 + t; i < nx; i += nt) {
+    const double dd = enew[i] - eorg[i];
+    const double bb = 0.5 * (bt[i - 1] + bt[i]);
+    fbt[i] = enew[i];
+    fen[i] += dd * bb;
+  }
 }
 
 }  // namespace qas

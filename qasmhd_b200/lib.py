@@ -13,7 +13,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libqas.so")
+# QASMHD_LIB: path of another build of the library (e.g. one compiled with other tuning macros)
+LIB_PATH = os.environ.get("QASMHD_LIB") or os.path.join(HERE, "libqas.so")
 
 # qas_status values
 QAS_OK = 0

@@ -177,13 +177,15 @@ def brio_wu(nxm: int = 1024, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3,
 
 
 def hall_shock(nxm: int = 400, di: float = 1e-3, rmn: int = RMN_LHLLD, odr: int = 4, rk: int = 3,
-               tmax: float = 1.0, nout: int = 1) -> Problem:
+               tmax: float = 1.0, nout: int = 1, d_ele: float = 0.0) -> Problem:
     """Brio-Wu states of the Hall driver (1D/SERIAL/h-shock/mhd1d_init_.cpp, NUM 2) on
     x in [-0.5, 0.5] split at x <= 0, gamma = 2, Neumann (+1) boundaries for every field
-    (hmhd1d_paras.cpp:6-20), ion inertia length di, no electron inertia (D_ELE = 0), and the
-    driver's exec_(0) loop (constant dt, h-shock/main.cpp)."""
+    (hmhd1d_paras.cpp:6-20), ion inertia length di, electron inertia length de = dx*d_ele (the
+    reference's D_ELE; 0 in its configurations), and the driver's exec_(0) loop (constant dt,
+    h-shock/main.cpp)."""
     p = Problem(name=f"hallshock_{nxm}", dim=1, nxm=nxm, rmn=rmn, odr=odr, rk=rk, ctw=0, gam=2.0, cfl=0.4,
                 dtrec=tmax, nout=nout, xmin=-0.5, xmax=0.5, dnx=(1,) * NM, flg=0, hall=True, di=di, de=0.0)
+    p.de = p.dx * d_ele
     x, _, _ = p.coords()
     left = x <= 0
     ro = np.where(left, 1.0, 0.125)

@@ -109,6 +109,7 @@ STEP_CASES = [
     ("bw1d_exec", lambda: P.brio_wu(64, tmax=0.02), R.MODE_EXEC, 0),
     ("hall1d_run", lambda: P.hall_shock(64, di=0.02), R.MODE_RUN, 6),
     ("hall1d_exec", lambda: P.hall_shock(64, di=1e-3, tmax=0.02), R.MODE_EXEC, 0),
+    ("hall1d_de_run", lambda: P.hall_shock(64, di=0.01, d_ele=2.0), R.MODE_RUN, 4),
     *[(f"ot2d_rmn{r}", (lambda r=r: P.orszag_tang(16, rmn=r)), R.MODE_RUN, 3) for r in range(4)],
     ("ot2d_ctw0", lambda: P.orszag_tang(16, ctw=0), R.MODE_RUN, 3),
     *[(f"ot2d_odr{o}", (lambda o=o: P.orszag_tang(16, odr=o, rk=min(o, 3))), R.MODE_RUN, 3) for o in (1, 2, 3)],

@@ -99,11 +99,13 @@ def test_live_reference_gravity(restatement, dim, ctw, rmn):
 
 
 @pytest.mark.skipif(not R.reference_available(1, 0, gravity="hall"), reason="reference Hall build not built")
-@pytest.mark.parametrize("di,odr", [(1e-3, 4), (0.05, 4), (0.02, 2)])
-def test_live_reference_hall(restatement, di, odr):
+@pytest.mark.parametrize("di,odr,d_ele", [(1e-3, 4, 0.0), (0.05, 4, 0.0), (0.02, 2, 0.0), (0.01, 4, 2.0),
+                                          (0.0, 4, 3.0)])
+def test_live_reference_hall(restatement, di, odr, d_ele):
     """The 1D Hall driver (1D/SERIAL/h-shock, HMHD1D): one hall_ call, and runs with the Hall
-    sub-cycles of exec_ (di = 0.05 gives tens of sub-cycles per step)."""
-    p = P.hall_shock(64, di=di, odr=odr, rk=3 if odr == 4 else 2)
+    sub-cycles of exec_ (di = 0.05 gives tens of sub-cycles per step); d_ele > 0 adds the
+    electron-inertia CG correction (crcte) to ideal() and hall_()."""
+    p = P.hall_shock(64, di=di, odr=odr, rk=3 if odr == 4 else 2, d_ele=d_ele)
     a = R.run_reference(p, R.MODE_DSTEP, dt=1e-3, nthreads=1)
     b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=1e-3)
     assert_bitwise(b["state"], a["state"], "hall_")

@@ -319,18 +319,19 @@ def test_gravity_forms_and_switch(restatement):
 
 
 
-@pytest.mark.parametrize("di,odr", [(1e-3, 4), (0.05, 4), (0.02, 3)])
-def test_hall_vs_oracle(restatement, di, odr):
+@pytest.mark.parametrize("di,odr,d_ele", [(1e-3, 4, 0.0), (0.05, 4, 0.0), (0.02, 3, 0.0), (0.01, 4, 2.0),
+                                          (0.0, 4, 1.0), (0.02, 2, 1.0)])
+def test_hall_vs_oracle(restatement, di, odr, d_ele):
     """Hall form of the 1D driver (qas_set_hall): one hall_ call, runs with Hall sub-cycles, and
-    the exec_(0) loop of the driver."""
-    p = P.hall_shock(128, di=di, odr=odr, rk=3)
+    the exec_(0) loop of the driver; with d_ele > 0 the electron-inertia CG correction too."""
+    p = P.hall_shock(128, di=di, odr=odr, rk=3, d_ele=d_ele)
     a = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=1e-3)
     b = run_gpu(p, R.MODE_DSTEP, dt=1e-3)
     assert_bitwise(b["state"], a["state"], "hall_")
     a = restatement.run(p, 5, mode=R.MODE_RUN)
     b = run_gpu(p, R.MODE_RUN, 5)
     assert_bitwise(b["state"], a["state"], "hall run")
-    q = P.hall_shock(128, di=di, odr=odr, tmax=0.01)
+    q = P.hall_shock(128, di=di, odr=odr, tmax=0.01, d_ele=d_ele)
     a = restatement.run(q, 0, mode=R.MODE_EXEC)
     b = run_gpu(q, R.MODE_EXEC)
     assert b["steps"] == a["steps"]
@@ -343,7 +344,7 @@ def test_hall_rejects_unsupported():
             ctx.set_hall(1e-3)
         with pytest.raises(L.QasError):
             ctx.hall(1e-3)
-    with L.Context.from_problem(P.brio_wu(32)) as ctx:
+    with L.Context.from_problem(P.orszag_tang(16)) as ctx:
         with pytest.raises(L.QasError) as e:
-            ctx.set_hall(1e-3, 1e-2)  # electron inertia: the correction solve is not built
+            ctx.set_hall(1e-3, 1e-2)  # the Hall driver is 1D
         assert e.value.status == L.QAS_ERR_UNSUPPORTED
