@@ -111,6 +111,11 @@ qas_status qas_cells(const qas_ctx *ctx, long long *nd);
  * to / from the device.  Replaces the host-resident state of common/mhd_class.hpp:32-42. */
 qas_status qas_upload(qas_ctx *ctx, double *const val[8]);
 qas_status qas_download(qas_ctx *ctx, double *val[8]);
+/* The derived arrays of common/mhd_class.hpp:34-37 (vx, vy, vz, pr into prim[0..3]; cell-centre
+ * cx, cy, cz into cc[0..2]; NULL arrays or entries are skipped), evaluated from the current state
+ * as prmtv() does at the start of ideal(): cell-centre B by fcen[ODR-1] with its ghost fill, then
+ * v = m/ro, p from the energy (the gravity form subtracts ro*phi_g; the state is not modified). */
+qas_status qas_primitives(qas_ctx *ctx, double *prim[4], double *cc[3]);
 /* Same with one contiguous host block of 8*nd doubles (field m at block + m*nd). */
 qas_status qas_upload_block(qas_ctx *ctx, const double *block);
 qas_status qas_download_block(qas_ctx *ctx, double *block);
@@ -151,6 +156,15 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * qas_dsptv is one dsptv(dt) call (no ghost fill before).  2D and 3D (QAS_ERR_UNSUPPORTED
  * in 1D, which has no dissipative driver in the reference). */
 qas_status qas_dissipate(qas_ctx *ctx, double dt, double nu0, double eta0);
+/* Per-cell viscosity and resistivity profiles (the API's nu/eta arrays, common/mhd_class.hpp:
+ * nd doubles each, host, reference layout; NULL for one of them = zero), as the reconnection
+ * drivers' setdc fills them (2D/SERIAL/MRX/dmhd2d_init_.cpp:85-106, 3D/MPI/MRX/dmhd3d_init_.cpp:
+ * 98-127): once installed, the dissipative step uses them -- rnu = 0.5*(ro*nu at the two cells),
+ * eta averaged over the four cells around each edge, the sub-cycle count from their maximum of
+ * max(2 nu, eta) -- and runs after every ideal step of qas_run; the scalar nu0/eta0 of the run
+ * options and of qas_dissipate/qas_dsptv must then be 0 (QAS_ERR_INVALID otherwise).  Both
+ * NULL removes them.  2D/3D only; a gravity context refuses them (no such driver). */
+qas_status qas_set_dissipation(qas_ctx *ctx, const double *nu, const double *eta);
 qas_status qas_dsptv(qas_ctx *ctx, double dt, double nu0, double eta0);
 
 /* max over the interior of |D_x bx + D_y by + D_z bz| with the ODR-consistent

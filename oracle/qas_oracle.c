@@ -1624,7 +1624,10 @@ int qo_dsptv(const qo_grid *g, double *u, double dt, double nu0, double eta0)
   double *ex = xcalloc(nd), *ey = xcalloc(nd), *ez = xcalloc(nd);
   double *vx = xcalloc(nd), *vy = xcalloc(nd), *vz = xcalloc(nd), *nu = xcalloc(nd), *eta = xcalloc(nd);
   if (!ut || !fx || !fy || !ex || !ey || !ez || !vx || !vy || !vz || !nu || !eta) return -1;
-  for (ss = 0; ss < nd; ss++) { nu[ss] = nu0; eta[ss] = eta0; }
+  for (ss = 0; ss < nd; ss++) {  /* setdc: the given profiles, else uniform */
+    nu[ss] = g->nu ? g->nu[ss] : nu0;
+    eta[ss] = g->eta ? g->eta[ss] : eta0;
+  }
   pt_fn fc = face_to_centre(g->odr), df = first_diff(g->odr);
   double idx = 1.0 / g->dx, idy = 1.0 / g->dy;
   double dtdx = dt * idx, dtdy = dt * idy;
@@ -1714,7 +1717,10 @@ static int qo_dsptv3(const qo_grid *g, double *u, double dt, double nu0, double 
   double *ex = xcalloc(nd), *ey = xcalloc(nd), *ez = xcalloc(nd);
   double *vx = xcalloc(nd), *vy = xcalloc(nd), *vz = xcalloc(nd), *nu = xcalloc(nd), *eta = xcalloc(nd);
   if (!ut || !fx || !fy || !fz || !ex || !ey || !ez || !vx || !vy || !vz || !nu || !eta) return -1;
-  for (ss = 0; ss < nd; ss++) { nu[ss] = nu0; eta[ss] = eta0; }
+  for (ss = 0; ss < nd; ss++) {  /* setdc: the given profiles, else uniform */
+    nu[ss] = g->nu ? g->nu[ss] : nu0;
+    eta[ss] = g->eta ? g->eta[ss] : eta0;
+  }
   pt_fn fc = face_to_centre(g->odr), df = first_diff(g->odr);
   double idx = 1.0 / g->dx, idy = 1.0 / g->dy, idz = 1.0 / g->dz;
   double dtdx = dt * idx, dtdy = dt * idy, dtdz = dt * idz;
@@ -1823,8 +1829,14 @@ int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0
   if (g->dim < 2) return -1;
   double dx = g->dx, dy = g->dy;
   double dr = g->dim == 3 ? qmin(qmin(dx, dy), g->dz) : qmin(dx, dy);
-  double dcmax = qmax(2 * nu0, eta0);
-  if (dcmax < 0.0) dcmax = 0.0;
+  /* setdc's reduction (2D/SERIAL/MRX/dmhd2d_init_.cpp:85-106): max over every cell of
+   * max(2 nu, eta), from 0 */
+  double dcmax = 0.0;
+  geo e = mkgeo(g);
+  for (long ss = 0; ss < e.nd; ss++) {
+    double dtmp = qmax(2 * (g->nu ? g->nu[ss] : nu0), g->eta ? g->eta[ss] : eta0);
+    if (dtmp > dcmax) dcmax = dtmp;
+  }
   if (dcmax > 1e-15) {
     int ncmax = 1 + (int)(2 * (dcmax * dt) / (dr * dr));
     for (int nc = 0; nc < ncmax; nc++) {

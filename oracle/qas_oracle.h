@@ -29,6 +29,8 @@ typedef struct {
                           the gravity form of the 2D/3D drivers (2D/SERIAL/RTI, 3D/MPI/RTI) */
   double hall_de;      /* 1D Hall driver's electron inertia length de (absolute); when non-zero
                           the by/bz fluxes of ideal() and hall_() get the crcte correction */
+  const double *nu, *eta;  /* per-cell viscosity / resistivity of the dissipative drivers (the
+                              API's nu/eta, nd doubles each); NULL: uniform nu0/eta0 arguments */
 } qo_grid;
 
 /* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,

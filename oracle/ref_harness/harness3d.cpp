@@ -22,6 +22,7 @@ int qh_xmesh = 1, qh_ymesh = 1, qh_zmesh = 1, qh_nout = 1, qh_rmn = 1, qh_odr = 
 double qh_dtrec = 1.0, qh_cfl = 0.4;
 
 static double g_nu0 = 0.0, g_eta0 = 0.0;
+static const double *g_nu_arr = nullptr, *g_eta_arr = nullptr;  /* per-cell profiles, if given */
 
 #ifndef QAS_GRAVITY
 
@@ -34,8 +35,8 @@ double DMHD3D::setdc()
     for (int j = 0; j < ny; j++) {
       for (int i = 0; i < nx; i++) {
         int ss = nx * (ny * k + j) + i;
-        nu[ss] = g_nu0;
-        eta[ss] = g_eta0;
+        nu[ss] = g_nu_arr ? g_nu_arr[ss] : g_nu0;
+        eta[ss] = g_eta_arr ? g_eta_arr[ss] : g_eta0;
         dtmp = max(2 * nu[ss], eta[ss]);
         if (dtmp > dcmax) dcmax = dtmp;
       }
@@ -64,11 +65,16 @@ class RefHarness3D : public RefBase {
     for (int m = 0; m < nm; m++) { dnxs[m] = h.dnx[m]; dnys[m] = h.dny[m]; dnzs[m] = h.dnz[m]; }
     for (int m = 0; m < nm; m++) memcpy(val[m], data + (size_t)m * nd, sizeof(double) * nd);
 #ifdef QAS_GRAVITY
-    if (!h.has_phi) ref_die("the gravity build needs phi_g in the case");
+    if (!(h.has_phi & 1)) ref_die("the gravity build needs phi_g in the case");
     memcpy(phi_g, data + (size_t)8 * nd, sizeof(double) * nd);
 #else
-    if (h.has_phi) ref_die("phi_g given to a build without gravity");
+    if (h.has_phi & 1) ref_die("phi_g given to a build without gravity");
 #endif
+    if (h.has_phi & 2) {  /* per-cell nu, eta after the state (and phi_g) */
+      const size_t o = (size_t)(8 + (h.has_phi & 1)) * nd;
+      g_nu_arr = data + o;
+      g_eta_arr = data + o + nd;
+    }
   }
   void dissipate()
   {

@@ -39,7 +39,8 @@ struct RefCaseHeader {
   int32_t dim, nxm, nym, nzm;
   int32_t rmn, odr, rk, ctw;
   int32_t mode, nsteps, flg, nthreads;
-  int32_t nout, has_phi;  /* has_phi: nd doubles of phi_g follow the 8 state arrays */
+  int32_t nout, has_phi;  /* bit 0: nd doubles of phi_g follow the 8 state arrays;
+                             bit 1: then the nu and eta arrays (nd doubles each) */
   double gam, cfl, dtrec, dt;
   double xmin, xmax, ymin, ymax, zmin, zmax;
   double nu0, eta0;
@@ -77,7 +78,7 @@ static inline void ref_read_case(const char *path, RefCaseHeader *h, std::vector
   long nx = h->nxm + 8;
   long ny = h->dim >= 2 ? h->nym + 8 : 1;
   long nz = h->dim >= 3 ? h->nzm + 8 : 1;
-  size_t n = (size_t)((8 + (h->has_phi ? 1 : 0)) * nx * ny * nz);
+  size_t n = (size_t)((8 + ((h->has_phi & 1) ? 1 : 0) + ((h->has_phi & 2) ? 2 : 0)) * nx * ny * nz);
   data->resize(n);
   if (fread(data->data(), sizeof(double), n, f) != n) ref_die("short data");
   fclose(f);

@@ -51,6 +51,15 @@ def reference_available(dim: int = 2, ctw: int = 1, gravity: bool = False) -> bo
     return os.access(ref_binary(dim, ctw, gravity), os.X_OK)
 
 
+def _nu_eta(prob):
+    nu, eta = getattr(prob, "nu_arr", None), getattr(prob, "eta_arr", None)
+    if nu is None and eta is None:
+        return None
+    z = np.zeros(prob.nd)
+    return (np.ascontiguousarray(z if nu is None else nu, dtype=np.float64).reshape(-1),
+            np.ascontiguousarray(z if eta is None else eta, dtype=np.float64).reshape(-1))
+
+
 def _phi(prob) -> Optional[np.ndarray]:
     phi = getattr(prob, "phi", None)
     return None if phi is None else np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
@@ -62,9 +71,11 @@ def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nth
     st = np.ascontiguousarray(st, dtype=np.float64).reshape(8, -1)
     assert st.shape[1] == prob.nd, (st.shape, prob.nd)
     phi = _phi(prob)
+    nue = _nu_eta(prob)
+    flags = (0 if phi is None else 1) | (0 if nue is None else 2)
     hdr = _HDR.pack(MAGIC_IN, prob.dim, prob.nxm, prob.nym, prob.nzm,
                     prob.rmn, prob.odr, prob.rk, prob.ctw,
-                    mode, nsteps, prob.flg, nthreads, prob.nout, 0 if phi is None else 1,
+                    mode, nsteps, prob.flg, nthreads, prob.nout, flags,
                     prob.gam, prob.cfl, prob.dtrec, dt,
                     prob.xmin, prob.xmax, prob.ymin, prob.ymax, prob.zmin, prob.zmax,
                     # the Hall build reads (di, de) from the (nu0, eta0) fields
@@ -76,6 +87,9 @@ def write_case(path: str, prob, mode: int, nsteps: int = 0, dt: float = 0.0, nth
         if phi is not None:
             assert phi.size == prob.nd
             f.write(phi.tobytes())
+        if nue is not None:
+            f.write(nue[0].tobytes())
+            f.write(nue[1].tobytes())
 
 
 def read_result(path: str, prob):
@@ -203,7 +217,8 @@ class _OGrid(ctypes.Structure):
                 ("gam", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dz", ctypes.c_double),
                 ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8),
-                ("phi", ctypes.POINTER(ctypes.c_double)), ("hall_de", ctypes.c_double)]
+                ("phi", ctypes.POINTER(ctypes.c_double)), ("hall_de", ctypes.c_double),
+                ("nu", ctypes.POINTER(ctypes.c_double)), ("eta", ctypes.POINTER(ctypes.c_double))]
 
 
 class Restatement:
@@ -245,6 +260,11 @@ class Restatement:
             g.dnx[m], g.dny[m], g.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
         if getattr(prob, "hall", False):
             g.hall_de = float(prob.de)
+        nue = _nu_eta(prob)
+        if nue is not None:
+            g._nue_keep = nue
+            g.nu = nue[0].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            g.eta = nue[1].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         phi = _phi(prob)
         if phi is not None:
             g._phi_keep = phi  # the pointer below must outlive the call

@@ -99,6 +99,9 @@ struct qas_ctx {
   // and persistent grid size; lr_tma_ok = supported by this grid, lr_tma = in use
   bool lr_tma_ok = false, lr_tma = false;
   double *d_phi = nullptr;  // gravitational potential of the gravity drivers (qas_set_gravity)
+  // per-cell viscosity / resistivity (qas_set_dissipation) and their setdc maximum
+  double *d_nu = nullptr, *d_eta = nullptr;
+  double diss_dcmax = 0.0;
   // Hall driver (qas_set_hall): ion inertia length, whistler speed factor, haldt reduction
   bool hall = false;
   double hall_di = 0.0, hall_vphix = 0.0, hall_de = 0.0;
@@ -642,10 +645,13 @@ long long launch_dsptv(qas_ctx *c, int nc, double nu0, double eta0)
 
 // setdc + sub-cycled dsptv after ideal (dmhd2d_class.cpp:19-26, dmhd3d_class.cpp:20-28),
 // device-guarded
+bool diss_arrays(const qas_ctx *c) { return c->view.nu != nullptr; }
+
 long long launch_dissipate(qas_ctx *c, double nu0, double eta0)
 {
+  // setdc's maximum of max(2 nu, eta) over every cell: the installed profiles, else uniform
   const double dcmax0 = (2 * nu0 >= eta0) ? 2 * nu0 : eta0;
-  const double dcmax = dcmax0 > 0.0 ? dcmax0 : 0.0;
+  const double dcmax = diss_arrays(c) ? c->diss_dcmax : (dcmax0 > 0.0 ? dcmax0 : 0.0);
   if (!(dcmax > 1e-15)) return 0;
   const double idz = c->grid.dim == 3 ? 1.0 / c->grid.dz : 0.0;
   QL(c, KID_DSUB, k_dsub_setup<<<1, 1, 0, c->stream>>>(c->view, c->d_dctl, dcmax, c->dr, 1.0 / c->grid.dx,
@@ -731,7 +737,7 @@ long long launch_exec_step(qas_ctx *c, const qas_run_opts &o, int n_after)
   QL(c, KID_BOUND, k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view));
   if (hall_active(c)) nk += launch_hall_subcycles(c, o.cfl);
   nk += 2 + launch_ideal(c);
-  if (c->grid.dim >= 2 && (o.nu0 > 0.0 || o.eta0 > 0.0)) nk += launch_dissipate(c, o.nu0, o.eta0);
+  if (c->grid.dim >= 2 && (o.nu0 > 0.0 || o.eta0 > 0.0 || diss_arrays(c))) nk += launch_dissipate(c, o.nu0, o.eta0);
   if (o.flg && (n_after % 2 == 0)) nk += launch_setdt(c, o.cfl, o.stop_rule, o.dtrec, o.nout);
   return nk;
 }
@@ -916,6 +922,8 @@ qas_status qas_destroy(qas_ctx *c)
   if (c->d_dctl) cudaFree(c->d_dctl);
   if (c->d_scratch) cudaFree(c->d_scratch);
   if (c->d_phi) cudaFree(c->d_phi);
+  if (c->d_nu) cudaFree(c->d_nu);
+  if (c->d_eta) cudaFree(c->d_eta);
   if (c->d_hvmax) cudaFree(c->d_hvmax);
   if (c->h_hvmax) cudaFreeHost(c->h_hvmax);
   if (c->h_ctl) cudaFreeHost(c->h_ctl);
@@ -950,6 +958,30 @@ qas_status qas_download(qas_ctx *c, double *val[8])
   for (int m = 0; m < 8; m++) {
     if (!val[m]) return QAS_ERR_INVALID;
     QAS_CUDA(cudaMemcpyAsync(val[m], c->view.u[m], bytes, cudaMemcpyDeviceToHost, c->stream));
+  }
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  return QAS_OK;
+}
+
+qas_status qas_primitives(qas_ctx *c, double *prim[4], double *cc[3])
+{
+  if (!c) return QAS_ERR_INVALID;
+  const Geo &g = c->geo;
+  const dim3 t = c->tile[KID_PRIM];
+  switch (c->scheme.odr) {
+    case 1: k_prim_eval<1><<<cells_grid(g, t), t, 0, c->stream>>>(c->view); break;
+    case 2: k_prim_eval<2><<<cells_grid(g, t), t, 0, c->stream>>>(c->view); break;
+    case 3: k_prim_eval<3><<<cells_grid(g, t), t, 0, c->stream>>>(c->view); break;
+    default: k_prim_eval<4><<<cells_grid(g, t), t, 0, c->stream>>>(c->view); break;
+  }
+  c->launches++;
+  qas_status s = check_launch(c);
+  if (s != QAS_OK) return s;
+  const size_t bytes = (size_t)g.nd * sizeof(double);
+  double *src[7] = {c->view.vx, c->view.vy, c->view.vz, c->view.pr, c->view.cx, c->view.cy, c->view.cz};
+  for (int m = 0; m < 7; m++) {
+    double *dst = m < 4 ? (prim ? prim[m] : nullptr) : (cc ? cc[m - 4] : nullptr);
+    if (dst) QAS_CUDA(cudaMemcpyAsync(dst, src[m], bytes, cudaMemcpyDeviceToHost, c->stream));
   }
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   return QAS_OK;
@@ -1046,6 +1078,7 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
   if (o.stop_rule < 0 || o.stop_rule > 2) return QAS_ERR_INVALID;
   if (o.stop_rule == 0 && o.max_steps <= 0) return QAS_ERR_INVALID;
   if ((o.nu0 > 0.0 || o.eta0 > 0.0) && (c->grid.dim < 2 || c->view.phi)) return QAS_ERR_UNSUPPORTED;
+  if (diss_arrays(c) && (o.nu0 != 0.0 || o.eta0 != 0.0)) return QAS_ERR_INVALID;  // one source of coefficients
   qas_status s;
   if (!c->run_initialised) {
     // setdt(1) of main(): dt and nmax from the initial state
@@ -1140,6 +1173,7 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
+  if (diss_arrays(c) && (nu0 != 0.0 || eta0 != 0.0)) return QAS_ERR_INVALID;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   const Geo &g = c->geo;
   const double idx = 1.0 / c->grid.dx, idy = 1.0 / c->grid.dy;
@@ -1178,6 +1212,7 @@ qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
 {
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
+  if (diss_arrays(c) && (nu0 != 0.0 || eta0 != 0.0)) return QAS_ERR_INVALID;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
   c->launches += 1 + launch_dissipate(c, nu0, eta0);
@@ -1287,6 +1322,45 @@ qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas
   }
   *count = w;
   return read_ctl(c);
+}
+
+qas_status qas_set_dissipation(qas_ctx *c, const double *nu, const double *eta)
+{
+  if (!c) return QAS_ERR_INVALID;
+  if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
+  QAS_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->graph) {  // captured launches carry the view by value
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if (!nu && !eta) {
+    c->view.nu = c->view.eta = nullptr;
+    return QAS_OK;
+  }
+  const size_t nd = (size_t)c->geo.nd, bytes = nd * sizeof(double);
+  if (!c->d_nu && cudaMalloc(&c->d_nu, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return QAS_ERR_NOMEM;
+  }
+  if (!c->d_eta && cudaMalloc(&c->d_eta, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return QAS_ERR_NOMEM;
+  }
+  std::vector<double> zero;
+  if (!nu || !eta) zero.assign(nd, 0.0);
+  const double *hn = nu ? nu : zero.data(), *he = eta ? eta : zero.data();
+  // setdc's reduction (2D/SERIAL/MRX/dmhd2d_init_.cpp:85-106): dtmp = max(2 nu, eta) per cell
+  double dcmax = 0.0;
+  for (size_t q = 0; q < nd; q++) {
+    const double dtmp = (2 * hn[q] >= he[q]) ? 2 * hn[q] : he[q];
+    if (dtmp > dcmax) dcmax = dtmp;
+  }
+  QAS_CUDA(cudaMemcpy(c->d_nu, hn, bytes, cudaMemcpyHostToDevice));
+  QAS_CUDA(cudaMemcpy(c->d_eta, he, bytes, cudaMemcpyHostToDevice));
+  c->view.nu = c->d_nu;
+  c->view.eta = c->d_eta;
+  c->diss_dcmax = dcmax;
+  return QAS_OK;
 }
 
 qas_status qas_set_hall(qas_ctx *c, double di, double de)

@@ -90,6 +90,14 @@ __global__ void k_eres(View v, const DCtl *dc, int nc, double eta0, double idx, 
   const double jy = dbxz * idz - dfc<ODR>(bz[c - 2], bz[c - 1], bz[c], bz[c + 1]) * idx;
   const double jz = dfc<ODR>(by[c - 2], by[c - 1], by[c], by[c + 1]) * idx -
                     dfc<ODR>(bx[c - 2 * sy], bx[c - sy], bx[c], bx[c + sy]) * idy;
+  if (v.eta) {  // per-cell resistivity averaged to the edges (mhd_func.c:103-105)
+    const double *et = v.eta;
+    const long long xo = 1, yo = sy, zo = g.dim == 3 ? g.s[2] : 0;
+    v.ex[c] = 0.25 * (et[c - yo - zo] + et[c - zo] + et[c - yo] + et[c]) * jx;
+    v.ey[c] = 0.25 * (et[c - zo - xo] + et[c - xo] + et[c - zo] + et[c]) * jy;
+    v.ez[c] = 0.25 * (et[c - xo - yo] + et[c - yo] + et[c - xo] + et[c]) * jz;
+    return;
+  }
   const double e = eta0;
   v.ex[c] = 0.25 * (e + e + e + e) * jx;
   v.ey[c] = 0.25 * (e + e + e + e) * jy;
@@ -175,7 +183,8 @@ __global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, 
   const double *ro = v.u[0];
   double fmx, fmy, fmz, fenv, fby, fbz, fenr;
   // x face (dmhd2d_solve.cpp:70-82, dmhd3d_solve.cpp:72-84)
-  double rnu = 0.5 * (ro[c - 1] * nu0 + ro[c] * nu0);
+  const double *nua = v.nu;  // per-cell viscosity, or the uniform nu0
+  double rnu = nua ? 0.5 * (ro[c - 1] * nua[c - 1] + ro[c] * nua[c]) : 0.5 * (ro[c - 1] * nu0 + ro[c] * nu0);
   visc_flux<ODR>(v.vx, v.vy, v.vz, c, rnu, idx, idy, idz, 1, sy, sz, fmx, fmy, fmz, fenv);
   resist_flux<ODR>(v.u[5], v.u[6], v.ey, v.ez, c, 1, sy, sz, fby, fbz, fenr);
   v.f[0][0][c] = 0.0 + 0.0;
@@ -186,7 +195,7 @@ __global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, 
   v.f[0][6][c] = 0.0 + fbz;
   v.f[0][7][c] = fenv + fenr;
   // y face (dmhd2d_solve.cpp:83-94, dmhd3d_solve.cpp:86-97)
-  rnu = 0.5 * (ro[c - sy] * nu0 + ro[c] * nu0);
+  rnu = nua ? 0.5 * (ro[c - sy] * nua[c - sy] + ro[c] * nua[c]) : 0.5 * (ro[c - sy] * nu0 + ro[c] * nu0);
   visc_flux<ODR>(v.vy, v.vz, v.vx, c, rnu, idy, idz, idx, sy, sz, 1, fmx, fmy, fmz, fenv);
   resist_flux<ODR>(v.u[6], v.u[4], v.ez, v.ex, c, sy, sz, 1, fby, fbz, fenr);
   v.f[1][0][c] = 0.0 + 0.0;
@@ -197,7 +206,7 @@ __global__ void k_dflux(View v, const DCtl *dc, int nc, double nu0, double idx, 
   v.f[1][4][c] = 0.0 + fbz;
   v.f[1][7][c] = fenv + fenr;
   if (d3) {  // z face (dmhd3d_solve.cpp:99-110)
-    rnu = 0.5 * (ro[c - sz] * nu0 + ro[c] * nu0);
+    rnu = nua ? 0.5 * (ro[c - sz] * nua[c - sz] + ro[c] * nua[c]) : 0.5 * (ro[c - sz] * nu0 + ro[c] * nu0);
     visc_flux<ODR>(v.vz, v.vx, v.vy, c, rnu, idz, idx, idy, sz, 1, sy, fmx, fmy, fmz, fenv);
     resist_flux<ODR>(v.u[4], v.u[5], v.ex, v.ey, c, sz, 1, sy, fby, fbz, fenr);
     v.f[2][0][c] = 0.0 + 0.0;

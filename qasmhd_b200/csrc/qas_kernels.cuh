@@ -68,6 +68,9 @@ struct View {
   // (2-gam)/(gam-1) of their boundary energy rule
   const double *phi;
   double gfac;
+  // per-cell viscosity / resistivity of the dissipative drivers (the API's nu/eta), or null
+  // for the uniform nu0/eta0 of the run options
+  const double *nu, *eta;
 };
 
 __device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
@@ -120,7 +123,9 @@ __device__ __forceinline__ bool interior_cell(const Geo &g, int i, int j, int k)
 // ---------------------------------------------------------------------------
 // primitives + cell-centre B (prmtv, bcell/bb2cc + bound(cx,cy,cz))
 // ---------------------------------------------------------------------------
-template <int ODR>
+// WB: store the gravity drivers' rounded energy back (the stage's prmtv); false for a read-only
+// evaluation of the primitives (qas_primitives)
+template <int ODR, bool WB = true>
 __device__ __forceinline__ void prim_body(const View &v, int i, int j, int k)
 {
   const Geo &g = v.g;
@@ -176,7 +181,7 @@ __device__ __forceinline__ void prim_body(const View &v, int i, int j, int k)
   const double v2 = vx * vx + vy * vy + vz * vz;
   const double b2 = cx * cx + cy * cy + cz * cz;
   const double pr = (v.gam - 1) * (en - 0.5 * (ro * v2 + b2));
-  if (v.phi) v.u[7][c] = en + ro * v.phi[c];
+  if (WB && v.phi) v.u[7][c] = en + ro * v.phi[c];
   v.vx[c] = vx;
   v.vy[c] = vy;
   v.vz[c] = vz;
@@ -195,6 +200,13 @@ __global__ void k_prim(View v)
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
   prim_body<ODR>(v, i, j, k);
+}
+// the primitives of the current state without touching it (no stop-flag guard)
+template <int ODR>
+__global__ void k_prim_eval(View v)
+{
+  QAS_CELL_INDEX();
+  prim_body<ODR, false>(v, i, j, k);
 }
 
 // ---------------------------------------------------------------------------

@@ -40,7 +40,7 @@ EXPORTS = (
     "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
     "qas_bkup_load", "qas_dd_plan", "qas_dd_create", "qas_dd_destroy", "qas_dd_upload_block",
     "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches", "qas_set_gravity",
-    "qas_set_hall", "qas_hall",
+    "qas_set_hall", "qas_hall", "qas_set_dissipation", "qas_primitives",
 )
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
@@ -170,6 +170,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_dd_destroy.argtypes = [vp]
     lib.qas_set_gravity.argtypes = [vp, dp]
     lib.qas_set_hall.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    lib.qas_set_dissipation.argtypes = [vp, dp, dp]
+    lib.qas_primitives.argtypes = [vp, ctypes.POINTER(dp), ctypes.POINTER(dp)]
     lib.qas_hall.argtypes = [vp, ctypes.c_double]
     lib.qas_dd_upload_block.argtypes = [vp, dp]
     lib.qas_dd_download_block.argtypes = [vp, dp]
@@ -227,7 +229,32 @@ class Context:
             ctx.set_gravity(prob.phi)
         if getattr(prob, "hall", False):
             ctx.set_hall(prob.di, prob.de)
+        if getattr(prob, "nu_arr", None) is not None or getattr(prob, "eta_arr", None) is not None:
+            ctx.set_dissipation(prob.nu_arr, prob.eta_arr)
         return ctx
+
+    def primitives(self, shape) -> dict:
+        """qas_primitives: vx, vy, vz, pr, cx, cy, cz of the current state (arrays of `shape`)."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        out = {k: np.empty(shape, dtype=np.float64) for k in ("vx", "vy", "vz", "pr", "cx", "cy", "cz")}
+        prim = (dp * 4)(*[_dptr(out[k]) for k in ("vx", "vy", "vz", "pr")])
+        cc = (dp * 3)(*[_dptr(out[k]) for k in ("cx", "cy", "cz")])
+        _check(self.lib.qas_primitives(self.h, prim, cc), "qas_primitives")
+        return out
+
+    def set_dissipation(self, nu: Optional[np.ndarray], eta: Optional[np.ndarray]) -> None:
+        """qas_set_dissipation: per-cell viscosity / resistivity profiles (None = zero; both None
+        removes them)."""
+        def arr(a):
+            if a is None:
+                return None, None
+            b = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+            if b.size != self.nd:
+                raise ValueError(f"profile has {b.size} values, the grid {self.nd}")
+            return b, _dptr(b)
+        kn, pn = arr(nu)
+        ke, pe = arr(eta)
+        _check(self.lib.qas_set_dissipation(self.h, pn, pe), "qas_set_dissipation")
 
     def set_hall(self, di: float, de: float = 0.0) -> None:
         """qas_set_hall: the Hall form of the 1D driver (ion / electron inertia lengths)."""

@@ -62,6 +62,9 @@ class Problem:
     state: Optional[np.ndarray] = None  # shape (8, nz, ny, nx) incl. ghosts
     # gravitational potential phi_g (nz, ny, nx) of the gravity drivers, None without gravity
     phi: Optional[np.ndarray] = None
+    # per-cell viscosity / resistivity of the dissipative drivers (the API's nu/eta), None: uniform
+    nu_arr: Optional[np.ndarray] = None
+    eta_arr: Optional[np.ndarray] = None
     # Hall driver (1D/SERIAL/h-shock, HMHD1D): on/off, ion inertia length di, electron inertia
     # length de (absolute, = dx*D_ELE)
     hall: bool = False
@@ -116,6 +119,8 @@ class Problem:
         p = dataclasses.replace(self)
         p.state = None if self.state is None else self.state.copy()
         p.phi = None if self.phi is None else self.phi.copy()
+        p.nu_arr = None if self.nu_arr is None else self.nu_arr.copy()
+        p.eta_arr = None if self.eta_arr is None else self.eta_arr.copy()
         return p
 
 
@@ -173,6 +178,20 @@ def brio_wu(nxm: int = 1024, rmn: int = RMN_HLLD, odr: int = 4, rk: int = 3,
     by = np.where(left, 1.0, -1.0)
     st = _pack(ro, z, z, z, bx, by, z, pr, bx, by, z, p.gam)
     p.state = st.reshape(NM, 1, 1, p.nx)
+    return p
+
+
+def localized_dissipation(prob: Problem, nu0: float, eta0: float, lam: float = 1.0) -> Problem:
+    """The localized profiles of the reconnection drivers' setdc, nu = nu0 exp(-r/lambda) and
+    eta = eta0 exp(-r/lambda) with r = sqrt(x^2 + y^2) over every padded cell
+    (2D/SERIAL/MRX/dmhd2d_init_.cpp:85-106, 3D/MPI/MRX/dmhd3d_init_.cpp:98-118); returns a copy
+    of the problem carrying them."""
+    p = prob.copy()
+    x, y, z = p.coords()
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    r = np.sqrt(X * X + Y * Y)
+    p.nu_arr = nu0 * np.exp(-r / lam)
+    p.eta_arr = eta0 * np.exp(-r / lam)
     return p
 
 

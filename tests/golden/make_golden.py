@@ -117,6 +117,9 @@ STEP_CASES = [
     ("kh2d_mlau", lambda: P.kelvin_helmholtz(2, 16, mach=0.3, rmn=P.RMN_MLAU), R.MODE_RUN, 3),
     ("kh2d_roe_eta", _kh2_eta, R.MODE_DRUN, 3),
     ("wave3d_eta_ctw1", lambda: _wave3_eta(1, 0.02, 0.05), R.MODE_DRUN, 2),
+    ("ot2d_profile_eta", lambda: P.localized_dissipation(P.orszag_tang(16), 0.01, 0.05, 0.5), R.MODE_DRUN, 3),
+    ("kh3d_profile_eta", lambda: P.localized_dissipation(P.kelvin_helmholtz(3, 8, mach=0.3, rmn=P.RMN_HLLD),
+                                                        0.01, 0.08, 0.3), R.MODE_DRUN, 2),
     ("wave3d_eta_ctw0_sub2", lambda: _wave3_eta(0, 0.05, 0.3, rmn=P.RMN_ROE), R.MODE_DRUN, 2),
     ("rt2d_lhlld", lambda: P.rayleigh_taylor(2, 16, 32), R.MODE_RUN, 3),
     ("rt2d_mlau_exec", lambda: P.rayleigh_taylor(2, 16, 32, rmn=P.RMN_MLAU, tmax=0.03), R.MODE_EXEC, 0),

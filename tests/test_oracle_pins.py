@@ -112,3 +112,17 @@ def test_live_reference_hall(restatement, di, odr, d_ele):
     a = R.run_reference(p, R.MODE_RUN, nsteps=4, nthreads=1)
     b = restatement.run(p, 4, mode=R.MODE_RUN)
     assert_bitwise(b["state"], a["state"], "hall run")
+
+
+@needs_ref
+@pytest.mark.parametrize("dim", [2, 3])
+def test_live_reference_dissipation_profiles(restatement, dim):
+    """Per-cell nu/eta of the reconnection drivers' setdc (localized exp(-r/lambda) profiles)."""
+    base = P.orszag_tang(24) if dim == 2 else P.kelvin_helmholtz(3, 10, mach=0.3, rmn=P.RMN_HLLD)
+    p = P.localized_dissipation(base, 0.01, 0.06, 0.4)
+    a = R.run_reference(p, R.MODE_DSTEP, dt=2e-3, nthreads=2)
+    b = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
+    assert_bitwise(b["state"], a["state"], "dsptv profiles")
+    a = R.run_reference(p, R.MODE_DRUN, nsteps=3, nthreads=2)
+    b = restatement.run(p, 3, mode=R.MODE_DRUN)
+    assert_bitwise(b["state"], a["state"], "drun profiles")

@@ -348,3 +348,48 @@ def test_hall_rejects_unsupported():
         with pytest.raises(L.QasError) as e:
             ctx.set_hall(1e-3, 1e-2)  # the Hall driver is 1D
         assert e.value.status == L.QAS_ERR_UNSUPPORTED
+
+
+
+@pytest.mark.parametrize("dim,use_graph", [(2, True), (2, False), (3, True)])
+def test_dissipation_profiles(restatement, dim, use_graph):
+    """Per-cell nu/eta (qas_set_dissipation): one dsptv call and the dissipative exec_ loop."""
+    base = P.orszag_tang(48) if dim == 2 else P.kelvin_helmholtz(3, 16, mach=0.3, rmn=P.RMN_HLLD)
+    p = P.localized_dissipation(base, 0.01, 0.06, 0.4)
+    a = restatement.run(p, 1, mode=R.MODE_DSTEP, dt=2e-3)
+    b = run_gpu(p, R.MODE_DSTEP, dt=2e-3)
+    assert_bitwise(b["state"], a["state"], "dsptv profiles")
+    a = restatement.run(p, 4, mode=R.MODE_DRUN)
+    b = run_gpu(p, R.MODE_DRUN, 4, use_graph=use_graph)
+    assert_bitwise(b["state"], a["state"], "drun profiles")
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        with pytest.raises(L.QasError) as e:  # one source of coefficients at a time
+            ctx.run(max_steps=1, flg=1, stop_rule=0, cfl=p.cfl, nu0=1e-3)
+        assert e.value.status == L.QAS_ERR_INVALID
+
+
+@pytest.mark.parametrize("grav", [False, True])
+def test_primitives_readback(grav):
+    """qas_primitives: prmtv of the current state (interior cells checked against the same
+    formulas in numpy, op for op), without modifying the state in the gravity form."""
+    p = P.rayleigh_taylor(2, 32, 64) if grav else P.orszag_tang(32)
+    with L.Context.from_problem(p) as ctx:
+        ctx.upload(p.state)
+        ctx.run(max_steps=2, flg=1, stop_rule=0, cfl=p.cfl)
+        st = ctx.download(p.state.shape)
+        pv = ctx.primitives(p.state.shape[1:])
+        assert np.array_equal(ctx.download(p.state.shape), st)
+    s = st[:, 0]
+    j, i = slice(4, -4), slice(4, -4)
+    bx, by = s[4], s[5]
+    cx = 0.0625 * (9.0 * (bx[j, 4:-4] + bx[j, 5:-3]) - (bx[j, 3:-5] + bx[j, 6:-2]))
+    cy = 0.0625 * (9.0 * (by[4:-4, i] + by[5:-3, i]) - (by[3:-5, i] + by[6:-2, i]))
+    cz = s[6][j, i]
+    ro = s[0][j, i]
+    iro = 1.0 / ro
+    vx, vy, vz = s[1][j, i] * iro, s[2][j, i] * iro, s[3][j, i] * iro
+    en = s[7][j, i] - ro * p.phi[0][j, i] if grav else s[7][j, i]
+    pr = (p.gam - 1) * (en - 0.5 * (ro * (vx * vx + vy * vy + vz * vz) + (cx * cx + cy * cy + cz * cz)))
+    for name, ref in (("vx", vx), ("vy", vy), ("vz", vz), ("pr", pr), ("cx", cx), ("cy", cy), ("cz", cz)):
+        assert_bitwise(pv[name][0][j, i], ref, name)
