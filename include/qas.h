@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define QAS_ABI_VERSION 1
+#define QAS_ABI_VERSION 2
 
 typedef enum {
   QAS_OK = 0,
@@ -57,9 +57,15 @@ typedef struct {
  *   rmn: 0 Roe, 1 HLLD, 2 LHLLD, 3 MLAU  (riemann[] order, common/mhd_class.hpp:102-105)
  *   odr: 1..4 (interpol[ODR-1], l_interp, fcen, df1: common/mhd_class.hpp:107-113)
  *   rk : 1..3 SSP Runge-Kutta stages (rk_fac, mhd2d_solve.cpp:7)
- *   ctw: CUCT upwind weighting of the corner EMFs (mhd2d_solve.cpp:91-103) */
+ *   ctw: CUCT upwind weighting of the corner EMFs (mhd2d_solve.cpp:91-103)
+ *   char_mode: face-value reconstruction of mhd_lrstate (common/mhd_func.c:108-161): 0 in
+ *     characteristic variables with the mhd_eigen_mi/ae eigenvectors (the reference's active
+ *     code, default); 1 in primitive variables, each field on its own (mhd_reconst,
+ *     common/mhd_eigen.c:667-706, the reference's debug alternative).  Appended field: a
+ *     zero-initialised struct keeps the default. */
 typedef struct {
   int rmn, odr, rk, ctw;
+  int char_mode;
 } qas_scheme;
 
 /* Boundary flags per field and axis, the dnxs/dnys/dnzs arrays of common/mhd_class.hpp:40:

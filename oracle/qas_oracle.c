@@ -297,11 +297,17 @@ static void char_reconst(int fast, const double q[7][5], double bn, double gamma
 }
 
 /* face states: common/mhd_func.c:108-161 */
-static void face_states(const double q[7][5], double bn, double gamma, lr_fn lr, double *vl, double *vr)
+/* mhd_lrstate (common/mhd_func.c:108-161); prim: the reconstruction call replaced by the
+ * primitive-variable mhd_reconst (common/mhd_eigen.c:667-706) */
+static void face_states(const double q[7][5], double bn, double gamma, lr_fn lr, double *vl, double *vr, int prim)
 {
   const double eps = 1e-12;
-  int fast = (q[0][2] * (q[1][2] * q[1][2] + q[2][2] * q[2][2] + q[3][2] * q[3][2]) > gamma * q[6][2]);
-  char_reconst(fast, q, bn, gamma, lr, vl, vr);
+  if (prim) {
+    for (int n = 0; n < 7; n++) lr(&q[n][2], &vl[n], &vr[n]);
+  } else {
+    int fast = (q[0][2] * (q[1][2] * q[1][2] + q[2][2] * q[2][2] + q[3][2] * q[3][2]) > gamma * q[6][2]);
+    char_reconst(fast, q, bn, gamma, lr, vl, vr);
+  }
   if (vl[0] <= eps || vl[6] <= eps) {
     vl[0] = q[0][2];
     vl[1] = q[1][2];
@@ -1064,8 +1070,8 @@ static void sweep(const geo *e, const double *const *u, work *w, int axis)
         gather5(qr[0], ro, sr, s); gather5(qr[1], v[a], sr, s); gather5(qr[2], v[b], sr, s);
         gather5(qr[3], v[cc], sr, s); gather5(qr[4], c[b], sr, s); gather5(qr[5], c[cc], sr, s);
         gather5(qr[6], pr, sr, s);
-        face_states(ql, c[a][sl], g->gam, lr, vl, tmp);
-        face_states(qr, c[a][sr], g->gam, lr, tmp, vr);
+        face_states(ql, c[a][sl], g->gam, lr, vl, tmp, g->char_mode);
+        face_states(qr, c[a][sr], g->gam, lr, tmp, vr, g->char_mode);
         for (int m = 0; m < 7; m++) { L[m] = vl[m]; R[m] = vr[m]; }
         double bn = 0.5 * (bf[a][ssf] + bf[a][ssf]);
         double dvsd[2];
@@ -1973,7 +1979,7 @@ int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out
       double q[7][5];
       for (int v = 0; v < 7; v++)
         for (int m = 0; m < 5; m++) q[v][m] = a[5 * v + m];
-      face_states(q, a[35], a[36], nl_interp(func - 19), &o[0], &o[7]);
+      face_states(q, a[35], a[36], nl_interp(func - 19), &o[0], &o[7], 0);
     } else if (func == 30) {
       o[0] = cuct_weight(&a[3], &a[7], &a[11], &a[15], &a[19], 1, 2);
     } else if (func == 31) {

@@ -31,6 +31,7 @@ typedef struct {
                           the by/bz fluxes of ideal() and hall_() get the crcte correction */
   const double *nu, *eta;  /* per-cell viscosity / resistivity of the dissipative drivers (the
                               API's nu/eta, nd doubles each); NULL: uniform nu0/eta0 arguments */
+  int char_mode;       /* 0 characteristic reconstruction (mhd_m/a_reconst), 1 primitive (mhd_reconst) */
 } qo_grid;
 
 /* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,

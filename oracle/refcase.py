@@ -37,10 +37,14 @@ MAGIC_IN = 0x31534151
 MAGIC_OUT = 0x32534151
 
 
-def ref_binary(dim: int, ctw: int, gravity: bool = False) -> str:
-    """The reference build for a case: ref1d, ref{2,3}d_ctw*, or the gravity drivers
-    (2D/SERIAL/RTI, 3D/MPI/RTI) ref{2,3}d_g_ctw*."""
-    if dim == 1:
+def ref_binary(dim: int, ctw: int, gravity=False) -> str:
+    """The reference build for a case: ref1d, ref{2,3}d_ctw*, the gravity drivers
+    (2D/SERIAL/RTI, 3D/MPI/RTI) ref{2,3}d_g_ctw* (gravity=True), the Hall driver ref1d_hall
+    (gravity="hall"), or the primitive-reconstruction builds ref1d_prim / ref{2,3}d_prim_ctw1
+    (gravity="prim")."""
+    if gravity == "prim":
+        name = "ref1d_prim" if dim == 1 else f"ref{dim}d_prim_ctw{int(bool(ctw))}"
+    elif dim == 1:
         name = "ref1d_hall" if gravity == "hall" else "ref1d"
     else:
         name = f"ref{dim}d_{'g_' if gravity else ''}ctw{int(bool(ctw))}"
@@ -114,7 +118,13 @@ def read_result(path: str, prob):
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
                   state: Optional[np.ndarray] = None, timeout: float = 3600.0):
     """Run the reference's own code on ``prob`` and return its result dict."""
-    exe = ref_binary(prob.dim, prob.ctw, "hall" if getattr(prob, "hall", False) else _phi(prob) is not None)
+    if getattr(prob, "char_mode", 0):
+        variant = "prim"
+    elif getattr(prob, "hall", False):
+        variant = "hall"
+    else:
+        variant = _phi(prob) is not None
+    exe = ref_binary(prob.dim, prob.ctw, variant)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"reference oracle binary missing: {exe} (build with `make -C oracle ref`)")
     with tempfile.TemporaryDirectory(prefix="qasref_") as td:
@@ -218,7 +228,8 @@ class _OGrid(ctypes.Structure):
                 ("dz", ctypes.c_double),
                 ("dnx", ctypes.c_int * 8), ("dny", ctypes.c_int * 8), ("dnz", ctypes.c_int * 8),
                 ("phi", ctypes.POINTER(ctypes.c_double)), ("hall_de", ctypes.c_double),
-                ("nu", ctypes.POINTER(ctypes.c_double)), ("eta", ctypes.POINTER(ctypes.c_double))]
+                ("nu", ctypes.POINTER(ctypes.c_double)), ("eta", ctypes.POINTER(ctypes.c_double)),
+                ("char_mode", ctypes.c_int)]
 
 
 class Restatement:
@@ -258,6 +269,7 @@ class Restatement:
         g.dz = prob.dz if prob.dim >= 3 else 0.0
         for m in range(8):
             g.dnx[m], g.dny[m], g.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])
+        g.char_mode = int(getattr(prob, "char_mode", 0))
         if getattr(prob, "hall", False):
             g.hall_de = float(prob.de)
         nue = _nu_eta(prob)

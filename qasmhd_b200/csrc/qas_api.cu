@@ -803,7 +803,7 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   if (gr.dim >= 3 && gr.nzm < 4) return QAS_ERR_INVALID;
   if (!(gr.dx > 0) || (gr.dim >= 2 && !(gr.dy > 0)) || (gr.dim >= 3 && !(gr.dz > 0))) return QAS_ERR_INVALID;
   if (scheme->rmn < 0 || scheme->rmn > 3 || scheme->odr < 1 || scheme->odr > 4 || scheme->rk < 1 ||
-      scheme->rk > 3)
+      scheme->rk > 3 || scheme->char_mode < 0 || scheme->char_mode > 1)
     return QAS_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return QAS_ERR_NO_DEVICE;
@@ -868,6 +868,7 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   v.odr = scheme->odr;
   v.rk = scheme->rk;
   v.ctw = scheme->ctw ? 1 : 0;
+  v.recon = scheme->char_mode;
   v.gam = gr.gam;
   v.dx = gr.dx;
   v.dy = gr.dim >= 2 ? gr.dy : 1.0;

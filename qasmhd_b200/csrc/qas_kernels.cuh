@@ -71,6 +71,7 @@ struct View {
   // per-cell viscosity / resistivity of the dissipative drivers (the API's nu/eta), or null
   // for the uniform nu0/eta0 of the run options
   const double *nu, *eta;
+  int recon;  // face-value reconstruction: 0 characteristic (mhd_m/a_reconst), 1 primitive (mhd_reconst)
 };
 
 __device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
@@ -279,11 +280,38 @@ struct LrStencil {
   __device__ __forceinline__ double late(int f, int m) const { return field(f)[c + (m - 2) * s]; }
 };
 
+// mhd_lrstate with the primitive reconstruction mhd_reconst (common/mhd_eigen.c:667-706): each
+// of (ro, vn, vb, vc, cb, cc, pr) interpolated on its own, then the positivity fallback
+// (common/mhd_func.c:150-160)
+template <int ODR, class ST>
+__device__ __forceinline__ void face_states_prim(const ST &st, double vl[7], double vr[7])
+{
+#pragma unroll
+  for (int f = 0; f < 7; f++) {
+    const double w[5] = {st(f, 0), st(f, 1), st(f, 2), st(f, 3), st(f, 4)};
+    nl_lr<ODR>(w, vl[f], vr[f]);
+  }
+  const double eps = 1e-12;
+  if (vl[0] <= eps || vl[6] <= eps) {
+    vl[0] = st(0, 2);
+    vl[1] = st(1, 2);
+    vl[6] = st(6, 2);
+  }
+  if (vr[0] <= eps || vr[6] <= eps) {
+    vr[0] = st(0, 2);
+    vr[1] = st(1, 2);
+    vr[6] = st(6, 2);
+  }
+}
+
 template <int ODR, int A, class ST>
 __device__ __forceinline__ void lr_cell(const View &v, long long c, long long s, const ST &st, double cnc)
 {
   double vl[7], vr[7];
-  face_states_grouped<ODR>(st, cnc, v.gam, vl, vr);
+  if (v.recon)
+    face_states_prim<ODR>(st, vl, vr);
+  else
+    face_states_grouped<ODR>(st, cnc, v.gam, vl, vr);
 #pragma unroll
   for (int m = 0; m < 7; m++) {
     v.vl[m][c] = vl[m];
@@ -441,7 +469,10 @@ __device__ __forceinline__ void cell_states(const View &v, long long c, double v
   const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
   const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
   const LrStencil<A> st{v, c, s};
-  face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
+  if (v.recon)
+    face_states_prim<ODR>(st, vl, vr);
+  else
+    face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
   if (g.dim >= 2) {
     const double *bnf = v.u[4 + A];
     const double bfl = __ldg(bnf + c + s), bfr = __ldg(bnf + c);

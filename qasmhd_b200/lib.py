@@ -63,8 +63,12 @@ class Grid(ctypes.Structure):
                 ("gam", ctypes.c_double)]
 
 
+ABI_VERSION = 2  # the layout of the structs below; qas_abi_version() of a matching libqas.so
+
+
 class Scheme(ctypes.Structure):
-    _fields_ = [("rmn", ctypes.c_int), ("odr", ctypes.c_int), ("rk", ctypes.c_int), ("ctw", ctypes.c_int)]
+    _fields_ = [("rmn", ctypes.c_int), ("odr", ctypes.c_int), ("rk", ctypes.c_int), ("ctw", ctypes.c_int),
+                ("char_mode", ctypes.c_int)]
 
 
 class BC(ctypes.Structure):
@@ -181,6 +185,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     for name in EXPORTS:
         if name not in ("qas_status_str", "qas_abi_version", "qas_last_cuda_error"):
             getattr(lib, name).restype = ctypes.c_int
+    if lib.qas_abi_version() != ABI_VERSION:
+        raise ImportError(f"{path} has ABI version {lib.qas_abi_version()}, the binding expects "
+                          f"{ABI_VERSION}: rebuild it with `python -m qasmhd_b200.build`")
     _lib = lib
     return lib
 
@@ -202,11 +209,11 @@ class Context:
 
     def __init__(self, dim: int, nxm: int, nym: int, nzm: int, dx: float, dy: float, dz: float, gam: float,
                  rmn: int, odr: int, rk: int, ctw: int, dnx: Sequence[int], dny: Sequence[int],
-                 dnz: Sequence[int], device: int = -1):
+                 dnz: Sequence[int], device: int = -1, char_mode: int = 0):
         self.lib = load()
         g = Grid(dim, nxm, nym if dim >= 2 else 1, nzm if dim >= 3 else 1, dx, dy if dim >= 2 else 0.0,
                  dz if dim >= 3 else 0.0, gam)
-        s = Scheme(rmn, odr, rk, ctw)
+        s = Scheme(rmn, odr, rk, ctw, char_mode)
         b = BC()
         for m in range(8):
             b.dnx[m], b.dny[m], b.dnz[m] = int(dnx[m]), int(dny[m]), int(dnz[m])
@@ -224,7 +231,7 @@ class Context:
         """A context for the problem; with gravity (prob.phi) the gravity form is switched on."""
         ctx = cls(prob.dim, prob.nxm, prob.nym, prob.nzm, prob.dx, prob.dy if prob.dim >= 2 else 0.0,
                   prob.dz if prob.dim >= 3 else 0.0, prob.gam, prob.rmn, prob.odr, prob.rk, prob.ctw,
-                  prob.dnx, prob.dny, prob.dnz, device)
+                  prob.dnx, prob.dny, prob.dnz, device, getattr(prob, "char_mode", 0))
         if getattr(prob, "phi", None) is not None:
             ctx.set_gravity(prob.phi)
         if getattr(prob, "hall", False):
@@ -534,7 +541,7 @@ class Decomposition:
 def _grid_scheme_bc(prob):
     g = Grid(prob.dim, prob.nxm, prob.nym if prob.dim >= 2 else 1, prob.nzm if prob.dim >= 3 else 1, prob.dx,
              prob.dy if prob.dim >= 2 else 0.0, prob.dz if prob.dim >= 3 else 0.0, prob.gam)
-    sc = Scheme(prob.rmn, prob.odr, prob.rk, prob.ctw)
+    sc = Scheme(prob.rmn, prob.odr, prob.rk, prob.ctw, getattr(prob, "char_mode", 0))
     b = BC()
     for m in range(8):
         b.dnx[m], b.dny[m], b.dnz[m] = int(prob.dnx[m]), int(prob.dny[m]), int(prob.dnz[m])

@@ -42,6 +42,7 @@ class Problem:
     odr: int = 4
     rk: int = 3
     ctw: int = 1
+    char_mode: int = 0  # face values in characteristic (0) or primitive (1) variables
     gam: float = 5.0 / 3.0
     cfl: float = 0.4
     dtrec: float = 1.0

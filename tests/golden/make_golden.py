@@ -90,6 +90,12 @@ def _wave3_eta(ctw, nu0, eta0, rmn=P.RMN_HLLD):
     return p
 
 
+def _prim(p):
+    """The primitive-variable reconstruction (mhd_reconst) instead of the characteristic one."""
+    p.char_mode = 1
+    return p
+
+
 def _wave_bc(dim, seed):
     rng = np.random.default_rng(seed)
 
@@ -108,6 +114,9 @@ STEP_CASES = [
     *[(f"bw1d_odr{o}", (lambda o=o: P.brio_wu(64, odr=o, rk=min(o, 3))), R.MODE_RUN, 5) for o in (1, 2, 3)],
     ("bw1d_exec", lambda: P.brio_wu(64, tmax=0.02), R.MODE_EXEC, 0),
     ("hall1d_run", lambda: P.hall_shock(64, di=0.02), R.MODE_RUN, 6),
+    ("bw1d_prim", lambda: _prim(P.brio_wu(64)), R.MODE_RUN, 5),
+    ("ot2d_prim", lambda: _prim(P.orszag_tang(16)), R.MODE_RUN, 3),
+    ("kh3d_prim", lambda: _prim(P.kelvin_helmholtz(3, 6, mach=0.3, rmn=P.RMN_MLAU)), R.MODE_RUN, 2),
     ("hall1d_exec", lambda: P.hall_shock(64, di=1e-3, tmax=0.02), R.MODE_EXEC, 0),
     ("hall1d_de_run", lambda: P.hall_shock(64, di=0.01, d_ele=2.0), R.MODE_RUN, 4),
     *[(f"ot2d_rmn{r}", (lambda r=r: P.orszag_tang(16, rmn=r)), R.MODE_RUN, 3) for r in range(4)],

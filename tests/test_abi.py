@@ -25,7 +25,8 @@ def test_library_exports_every_declared_symbol():
     lib = L.load()
     for name in declared_functions():
         assert hasattr(lib, name), name
-    assert lib.qas_abi_version() == 1
+    abi = int(re.search(r"#define QAS_ABI_VERSION (\d+)", open(os.path.join(ROOT, "include", "qas.h")).read())[1])
+    assert lib.qas_abi_version() == abi == L.ABI_VERSION
 
 
 def test_status_strings():

@@ -86,3 +86,17 @@ def test_batch_rejects_mixed_order():
     probs = [P.orszag_tang(16), P.orszag_tang(16, odr=2)]
     with pytest.raises(L.QasError):
         L.Batch(probs)
+
+
+def test_batch_mixed_reconstruction(restatement):
+    """Instances with characteristic and primitive-variable face values in one ensemble."""
+    probs = small_ensemble()[:4]
+    for q, p in enumerate(probs):
+        p.char_mode = q & 1
+    with L.Batch(probs) as b:
+        for q, p in enumerate(probs):
+            b.upload(q, p.state)
+        b.run(max_steps=3, flg=1, stop_rule=0, cfl=0.4)
+        outs = [b.download(q, p.state.shape) for q, p in enumerate(probs)]
+    for q, p in enumerate(probs):
+        assert_bitwise(outs[q], restatement.run(p, 3, mode=R.MODE_RUN)["state"], f"{p.name} char_mode {q & 1}")

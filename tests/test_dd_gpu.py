@@ -27,12 +27,18 @@ def _split(p, nparts, nsteps, stop_rule=0):
         return dd.download(), info, dd.kernel_launches()
 
 
+def _prim(p):
+    p.char_mode = 1
+    return p
+
+
 CASES = {
     "ot2d_64_hlld": lambda: P.orszag_tang(64),
     "ot2d_72_roe_ctw0": lambda: P.orszag_tang(72, rmn=P.RMN_ROE, ctw=0),
     "kh2d_64x48_mlau_open": lambda: P.kelvin_helmholtz(2, 64, nym=48, mach=0.3),
     "kh3d_16x16x32_mlau": lambda: P.kelvin_helmholtz(3, 16, nzm=32, mach=0.3),
     "kh3d_24_lhlld": lambda: P.kelvin_helmholtz(3, 24, mach=0.3, rmn=P.RMN_LHLLD),
+    "kh3d_16x16x24_prim": lambda: _prim(P.kelvin_helmholtz(3, 16, nzm=24, mach=0.3)),
     "wave3d_physical_z_roe": lambda: P.smooth_wave(3, 24, rmn=P.RMN_ROE,
                                                    dn=((0,) * 8, (0,) * 8, (2, 1, 1, -1, 1, 1, -1, 2))),
 }

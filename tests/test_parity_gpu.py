@@ -393,3 +393,23 @@ def test_primitives_readback(grav):
     pr = (p.gam - 1) * (en - 0.5 * (ro * (vx * vx + vy * vy + vz * vz) + (cx * cx + cy * cy + cz * cz)))
     for name, ref in (("vx", vx), ("vy", vy), ("vz", vz), ("pr", pr), ("cx", cx), ("cy", cy), ("cz", cz)):
         assert_bitwise(pv[name][0][j, i], ref, name)
+
+
+
+@pytest.mark.parametrize("case", ["bw1d", "ot2d", "kh3d_mlau", "ot2d_fused", "ot2d_staged"])
+def test_primitive_reconstruction(restatement, case):
+    """char_mode = 1: face values by mhd_reconst (each primitive on its own), every form."""
+    p = {"bw1d": lambda: P.brio_wu(128), "ot2d": lambda: P.orszag_tang(64, rmn=P.RMN_HLLD),
+         "kh3d_mlau": lambda: P.kelvin_helmholtz(3, 16, mach=0.3), "ot2d_fused": lambda: P.orszag_tang(64),
+         "ot2d_staged": lambda: P.orszag_tang(64)}[case]()
+    p.char_mode = 1
+    a = restatement.run(p, 4, mode=R.MODE_RUN)
+    with L.Context.from_problem(p) as ctx:
+        if case.endswith("fused"):
+            ctx.set_option(L.QAS_OPT_FUSED_SWEEP, 1)
+        if case.endswith("staged"):
+            ctx.set_option(L.QAS_OPT_LR_STAGING, 1)
+        ctx.upload(p.state)
+        ctx.run(max_steps=4, flg=p.flg, stop_rule=0, cfl=p.cfl, use_graph=not case.endswith("fused"))
+        b = ctx.download(p.state.shape)
+    assert_bitwise(b, a["state"], f"prim {case}")
