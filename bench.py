@@ -167,9 +167,38 @@ def cpu_baseline(prob, steps=3, threads=None):
     st = r["step_times"]
     per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
     return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
-            "kind": "reference",
+            "kind": "reference", "cpu": host_cpu(),
             "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, "
                       f"reference -O2 -fopenmp, OMP_NUM_THREADS={threads}"}
+
+
+def host_cpu() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_o3(prob, steps=3, threads=None):
+    """The same bounded sample through the reference built with its alternative flags
+    (Makefile.inc:3, -O3 -march=native: here the host's x86-64 ISA level).  Timing only: FMA
+    contraction changes its last bits."""
+    from oracle import refcase as R
+    threads = threads or os.cpu_count()
+    exe = R.o3_binary(prob.dim)
+    if exe is None:
+        return None
+    r = R.run_reference(prob, R.MODE_RUN, nsteps=steps, nthreads=threads, exe=exe)
+    st = r["step_times"]
+    per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
+    return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
+            "kind": "reference", "cpu": host_cpu(),
+            "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, reference "
+                      f"-O3 -march=x86-64-{R.host_isa_level()} -fopenmp, OMP_NUM_THREADS={threads}"}
 
 
 def ensemble_compare(steps):
@@ -249,14 +278,17 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
         prof = ctx.profile(2, flg=1, cfl=prob.cfl)
     gpu = prob.interior_cells / (ms * 1e-3) / 1e6
     cpu = cpu_baseline(prob, steps=cpu_steps) if cpu_steps > 0 else None
+    cpu3 = cpu_baseline_o3(prob, steps=cpu_steps) if cpu_steps > 0 else None
     out = {"workload": "kelvin_helmholtz_3d_256^3_M0.01_mlau_wcns4_ct_rk3", "value": gpu,
            "unit": "Mcell-updates/s", "ms_per_step": ms, "steps": steps,
            "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
-           "cpu_baseline": cpu,
+           "cpu_baseline": cpu, "cpu_baseline_o3": cpu3,
            "step_roofline": {"achieved": ALG_BYTES_PER_CELL_UPDATE * prob.interior_cells / (ms * 1e-3) / 1e9,
                              "unit": "GB/s", "basis": "512 algorithmic B per cell-update"}}
     if cpu:
         out["ratio_vs_cpu"] = gpu / cpu["value"]
+    if cpu3:
+        out["ratio_vs_cpu_o3"] = gpu / cpu3["value"]
     return out
 
 
@@ -358,6 +390,13 @@ def run_reference_arm(args):
             "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
                              "sample": f"{prob.name}: {args.warmup}+{len(st)} steps, reference -O2 -fopenmp"},
             "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    exe = R.o3_binary(prob.dim)
+    if exe:  # the same steps through the reference's alternative -O3 -march=native flags
+        r3 = R.run_reference(prob, R.MODE_RUN, nsteps=args.warmup + args.steps, nthreads=threads, exe=exe)
+        st3 = r3["step_times"][args.warmup:]
+        line["o3_native"] = {"value": prob.interior_cells * len(st3) / float(np.sum(st3)) / 1e6,
+                             "unit": "Mcell-updates/s", "cores": threads,
+                             "build": f"-O3 -march=x86-64-{R.host_isa_level()} -fopenmp (timing only)"}
     print(json.dumps(line))
 
 
@@ -502,6 +541,7 @@ def main():
     }
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(prob)
+        line["cpu_baseline_o3"] = cpu_baseline_o3(prob)
     if rank == 0 and not args.no_ensemble and world == 1:
         ctx.close()
         line["batched"] = ensemble_compare(args.ensemble_steps)

@@ -55,6 +55,35 @@ def reference_available(dim: int = 2, ctw: int = 1, gravity: bool = False) -> bo
     return os.access(ref_binary(dim, ctw, gravity), os.X_OK)
 
 
+def host_isa_level() -> str:
+    """x86-64 ISA level of this host for the -O3 timing builds: "v4" with AVX-512 (F, BW, CD,
+    DQ, VL), else "v3" with AVX2 + FMA + BMI2, else "" (no such build runs here)."""
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        return ""
+    if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags:
+        return "v4"
+    if {"avx2", "fma", "bmi2", "movbe"} <= flags:
+        return "v3"
+    return ""
+
+
+def o3_binary(dim: int) -> Optional[str]:
+    """The reference built with -O3 -march=<this host's ISA level> -fopenmp (CTW=1; timing
+    only), or None when there is none for this host."""
+    lvl = host_isa_level()
+    if not lvl or dim not in (2, 3):
+        return None
+    exe = os.path.join(REF_DIR, f"ref{dim}d_o3{lvl}_ctw1")
+    return exe if os.access(exe, os.X_OK) else None
+
+
 def _nu_eta(prob):
     nu, eta = getattr(prob, "nu_arr", None), getattr(prob, "eta_arr", None)
     if nu is None and eta is None:
@@ -116,15 +145,16 @@ def read_result(path: str, prob):
 
 
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
-                  state: Optional[np.ndarray] = None, timeout: float = 3600.0):
-    """Run the reference's own code on ``prob`` and return its result dict."""
+                  state: Optional[np.ndarray] = None, timeout: float = 3600.0, exe: Optional[str] = None):
+    """Run the reference's own code on ``prob`` and return its result dict (``exe``: another
+    build of the same driver, e.g. o3_binary(), for timing)."""
     if getattr(prob, "char_mode", 0):
         variant = "prim"
     elif getattr(prob, "hall", False):
         variant = "hall"
     else:
         variant = _phi(prob) is not None
-    exe = ref_binary(prob.dim, prob.ctw, variant)
+    exe = exe or ref_binary(prob.dim, prob.ctw, variant)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"reference oracle binary missing: {exe} (build with `make -C oracle ref`)")
     with tempfile.TemporaryDirectory(prefix="qasref_") as td:

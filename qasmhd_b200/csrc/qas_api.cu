@@ -438,9 +438,16 @@ void launch_lr(qas_ctx *c, int a)
     launch_lr_tma(c, a);
     return;
   }
-  if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
-  if (a == 1) QL(c, KID_LR, k_lr<ODR, 1><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
-  if (a == 2) QL(c, KID_LR, k_lr<ODR, 2><<<cells_grid(c->geo, c->tile[KID_LR]), c->tile[KID_LR], 0, c->stream>>>(c->view));
+  const dim3 grid = cells_grid(c->geo, c->tile[KID_LR]), blk = c->tile[KID_LR];
+  if (c->view.recon) {
+    if (a == 0) QL(c, KID_LR, k_lr<ODR, 0, 1><<<grid, blk, 0, c->stream>>>(c->view));
+    if (a == 1) QL(c, KID_LR, k_lr<ODR, 1, 1><<<grid, blk, 0, c->stream>>>(c->view));
+    if (a == 2) QL(c, KID_LR, k_lr<ODR, 2, 1><<<grid, blk, 0, c->stream>>>(c->view));
+    return;
+  }
+  if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<grid, blk, 0, c->stream>>>(c->view));
+  if (a == 1) QL(c, KID_LR, k_lr<ODR, 1><<<grid, blk, 0, c->stream>>>(c->view));
+  if (a == 2) QL(c, KID_LR, k_lr<ODR, 2><<<grid, blk, 0, c->stream>>>(c->view));
 }
 template <int RMN>
 void launch_flux(qas_ctx *c, int a)

@@ -304,11 +304,14 @@ __device__ __forceinline__ void face_states_prim(const ST &st, double vl[7], dou
   }
 }
 
-template <int ODR, int A, class ST>
+// PR: the face-value form, 0 characteristic, 1 primitive, -1 chosen at run time by v.recon (the
+// forms whose instances may differ per launch); the default kernels take it as a template
+// argument so the characteristic code is compiled without the other branch
+template <int ODR, int A, int PR = -1, class ST>
 __device__ __forceinline__ void lr_cell(const View &v, long long c, long long s, const ST &st, double cnc)
 {
   double vl[7], vr[7];
-  if (v.recon)
+  if (PR == 1 || (PR < 0 && v.recon))
     face_states_prim<ODR>(st, vl, vr);
   else
     face_states_grouped<ODR>(st, cnc, v.gam, vl, vr);
@@ -342,7 +345,7 @@ __device__ __forceinline__ void lr_cell(const View &v, long long c, long long s,
   }
 }
 
-template <int ODR, int A>
+template <int ODR, int A, int PR = -1>
 __device__ __forceinline__ void lr_body(const View &v, int i, int j, int k)
 {
   const Geo &g = v.g;
@@ -353,14 +356,14 @@ __device__ __forceinline__ void lr_body(const View &v, int i, int j, int k)
   const long long s = g.s[A];
   const double *cn = A == 0 ? v.cx : (A == 1 ? v.cy : v.cz);
   const LrStencil<A> st{v, c, s};
-  lr_cell<ODR, A>(v, c, s, st, cn[c]);
+  lr_cell<ODR, A, PR>(v, c, s, st, cn[c]);
 }
-template <int ODR, int A>
+template <int ODR, int A, int PR = 0>
 __global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
 {
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
-  lr_body<ODR, A>(v, i, j, k);
+  lr_body<ODR, A, PR>(v, i, j, k);
 }
 
 // ---------------------------------------------------------------------------

@@ -138,3 +138,15 @@ def test_live_reference_primitive_reconstruction(restatement, dim):
     a = R.run_reference(p, R.MODE_RUN, nsteps=3, nthreads=2)
     b = restatement.run(p, 3, mode=R.MODE_RUN)
     assert_bitwise(b["state"], a["state"], f"prim {dim}d")
+
+
+@pytest.mark.skipif(R.o3_binary(2) is None or R.o3_binary(3) is None, reason="no -O3 timing build for this host")
+@pytest.mark.parametrize("dim", [2, 3])
+def test_o3_timing_build_runs_the_same_case(dim):
+    """The -O3 -march timing build is the same driver: equal to round-off (FMA contraction),
+    not bitwise, so it never pins anything."""
+    p = P.orszag_tang(32) if dim == 2 else P.kelvin_helmholtz(3, 8, mach=0.3, rmn=P.RMN_MLAU)
+    a = R.run_reference(p, R.MODE_RUN, nsteps=3, nthreads=2)
+    b = R.run_reference(p, R.MODE_RUN, nsteps=3, nthreads=2, exe=R.o3_binary(dim))
+    scale = np.abs(a["state"]).max()
+    assert np.abs(a["state"] - b["state"]).max() <= 1e-9 * scale
