@@ -15,6 +15,35 @@
 
 #include "qas_device.cuh"
 
+// Resident-block caps of the memory-bound kernels (0: no launch bound, the compiler's choice).
+// Measured on B200 (OT 1024^2 / KH 160^3 per launch): k_update at 16 blocks (32 registers, a
+// few spills) 0.0887 -> 0.0804 ms / 0.383 -> 0.328 ms, k_prim at 16 0.125 -> 0.113 ms in 3D;
+// k_emf is slower capped (0.230 -> 0.250 ms at 12), so it keeps the compiler's choice.
+#ifndef QAS_PRIM_MINB
+#define QAS_PRIM_MINB 16
+#endif
+#ifndef QAS_EMF_MINB
+#define QAS_EMF_MINB 0
+#endif
+#ifndef QAS_UPDATE_MINB
+#define QAS_UPDATE_MINB 16
+#endif
+#if QAS_PRIM_MINB > 0
+#define QAS_PRIM_BOUNDS __launch_bounds__(128, QAS_PRIM_MINB)
+#else
+#define QAS_PRIM_BOUNDS
+#endif
+#if QAS_EMF_MINB > 0
+#define QAS_EMF_BOUNDS __launch_bounds__(128, QAS_EMF_MINB)
+#else
+#define QAS_EMF_BOUNDS
+#endif
+#if QAS_UPDATE_MINB > 0
+#define QAS_UPDATE_BOUNDS __launch_bounds__(128, QAS_UPDATE_MINB)
+#else
+#define QAS_UPDATE_BOUNDS
+#endif
+
 namespace qas {
 
 constexpr int GH = 4;  // ghost cells per side
@@ -196,7 +225,7 @@ __device__ __forceinline__ void prim_body(const View &v, int i, int j, int k)
   if (interior && !(ro > 0.0 && pr > 0.0 && isfinite(vx) && isfinite(vy) && isfinite(vz))) atomicOr(&v.ctl->err, 1);
 }
 template <int ODR>
-__global__ void k_prim(View v)
+__global__ void QAS_PRIM_BOUNDS k_prim(View v)
 {
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
@@ -251,8 +280,10 @@ __global__ void k_dv(View v)
 // ---------------------------------------------------------------------------
 // face states of each cell along axis A (mhd_lrstate + mhd_lr_fb)
 // ---------------------------------------------------------------------------
+// 6 resident blocks (80 registers, 52 B spilled to L1): 0.498 -> 0.478 ms per launch at KH 160^3,
+// unchanged in 2D; 5 blocks (96 registers) and 4 (118) are slower
 #ifndef QAS_LR_MINB
-#define QAS_LR_MINB 5
+#define QAS_LR_MINB 6
 #endif
 
 // stencil accessor of k_lr: field f of (ro, vn, vb, vc, cb, cc, pr) along axis A at point m
@@ -670,7 +701,7 @@ __device__ __forceinline__ void emf_body(const View &v, int i, int j, int k)
   }
 }
 template <int ODR>
-__global__ void k_emf(View v)
+__global__ void QAS_EMF_BOUNDS k_emf(View v)
 {
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
@@ -786,7 +817,7 @@ __device__ __forceinline__ bool update_cell(const Geo &g, int ti, int tj, int tk
 }
 
 template <int ODR>
-__global__ void k_update(View v, double c0, double c1)
+__global__ void QAS_UPDATE_BOUNDS k_update(View v, double c0, double c1)
 {
   if (v.ctl->done) return;
   int i, j, k;
