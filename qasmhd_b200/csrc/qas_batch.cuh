@@ -32,7 +32,7 @@ struct BMap {
 #define QAS_BATCH_CELL_OK (ti < v.g.nx && tj < v.g.ny && tk < v.g.nz)
 
 template <int ODR>
-__global__ void kb_prim(const View *__restrict__ views, BMap map)
+__global__ void QAS_PRIM_BOUNDS kb_prim(const View *__restrict__ views, BMap map)
 {
   QAS_BATCH_BLOCKS(map)
   if (QAS_BATCH_CELL_OK) prim_body<ODR>(v, ti, tj, tk);
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(128, QAS_LR_MINB) kb_lr(const View *__restrict
 }
 
 template <int RMN, int A>
-__global__ void __launch_bounds__(128) kb_flux(const View *__restrict__ views, BMap map)
+__global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) kb_flux(const View *__restrict__ views, BMap map)
 {
   QAS_BATCH_BLOCKS(map)
   if (QAS_BATCH_CELL_OK) {
@@ -89,7 +89,7 @@ __global__ void kb_emf(const View *__restrict__ views, BMap map)
 }
 
 template <int ODR>
-__global__ void kb_update(const View *__restrict__ views, BMap map, double c0, double c1)
+__global__ void QAS_UPDATE_BOUNDS kb_update(const View *__restrict__ views, BMap map, double c0, double c1)
 {
   QAS_BATCH_BLOCKS(map)
   int i, j, k;

@@ -453,8 +453,21 @@ __device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
   // work done by gravity (2D/SERIAL/RTI/mhd2d_solve.cpp:197, :305; 3D/MPI/RTI/mhd3d_solve.cpp:247, :412, :577)
   v.f[A][7][f] = v.phi ? F[6] + F[0] * 0.5 * (v.phi[f - s] + v.phi[f]) : F[6];
 }
+// resident-block caps of the flux kernel per solver, measured on B200 per launch: Roe at 4
+// (128 registers, from 162) 0.0906 -> 0.0782 ms (KH 2D 1024^2); HLLD at 8 (64 registers, a
+// few spills) 0.0525 -> 0.0501 ms (OT 1024^2); LHLLD at 8 0.181 -> 0.152 ms (KH 3D 128^3)
+#ifndef QAS_FLUX_ROE_MINB
+#define QAS_FLUX_ROE_MINB 4
+#endif
+#ifndef QAS_FLUX_HLLD_MINB
+#define QAS_FLUX_HLLD_MINB 8
+#endif
+#ifndef QAS_FLUX_LHLLD_MINB
+#define QAS_FLUX_LHLLD_MINB 8
+#endif
+#define QAS_FLUX_MINB_OF(RMN) ((RMN) == 0 ? QAS_FLUX_ROE_MINB : ((RMN) == 1 ? QAS_FLUX_HLLD_MINB : QAS_FLUX_LHLLD_MINB))
 template <int RMN, int A>
-__global__ void __launch_bounds__(128) k_flux(View v)
+__global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) k_flux(View v)
 {
   if (v.ctl->done) return;
   QAS_CELL_INDEX();
