@@ -40,7 +40,7 @@ K_LR_FP64_INSTR_PER_CELL = 1054.0
 K_LR_FP64_FLOPS_PER_CELL = 1262.0
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_lr launch (y direction) on the
 # same workload (profiles/k_lr_ot2d_1024.md)
-K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.76e6 + 99.48e6}
+K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.70e6 + 92.25e6}
 
 
 def parse():
