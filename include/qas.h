@@ -156,6 +156,18 @@ qas_status qas_run(qas_ctx *ctx, const qas_run_opts *opts, qas_run_info *info);
 /* Reset exec_'s counters (n = 0, tim = 0, setdt(1) pending) without touching the state. */
 qas_status qas_run_reset(qas_ctx *ctx);
 
+/* One exec_ step on host arrays: the same result, bits and loop state as qas_upload_block(in)
+ * + qas_run(opts, one step) + qas_download_block(out) -- the drop-in for a call of ideal()
+ * (mhd2d_solve.cpp:3-400 via exec_, mhd2d_class.cpp:35-61) on the caller's val[] arrays, which
+ * the reference updates in place (in == out is allowed).  In and out are blocks of 8*nd
+ * doubles in the qas_upload_block layout.  From the second step of a run on, 2D and 3D contexts
+ * without Hall, gravity or dissipation overlap the copies with the kernels: the last axis is
+ * processed in items (QAS_OPT_PIPE_ITEMS), the upload of later items runs beside the first
+ * stage of earlier ones and the download of finished items beside the last stage of later
+ * ones; pinned host memory is needed for the overlap.  The first such call allocates two
+ * stage buffers (16 doubles per cell).  opts->max_steps is ignored (one step). */
+qas_status qas_step_host(qas_ctx *ctx, const double *in, double *out, const qas_run_opts *opts, qas_run_info *info);
+
 /* Visco-resistive update with uniform coefficients: DMHD2D::setdc + the sub-cycled
  * dsptv of DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26, dmhd2d_solve.cpp:3-151),
  * and of DMHD3D::exec_ (3D/MPI/MRX/dmhd3d_class.cpp:20-28, dmhd3d_solve.cpp:3-179) in 3D.
@@ -236,6 +248,7 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
  * All forms give bit-identical results. */
 #define QAS_OPT_FUSED_SWEEP 1
 #define QAS_OPT_LR_STAGING 2
+#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 8) */
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

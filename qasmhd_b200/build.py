@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libqas.so")
 SOURCES = ["qas_api.cu"]
 HEADERS = ["qas_device.cuh", "qas_kernels.cuh", "qas_dissip.cuh", "qas_batch.cuh", "qas_batch_api.inc",
            "qas_adjoint.cuh", "qas_adjoint_kernels.cuh", "qas_adjoint_api.inc", "qas_noalloc.inc",
-           "qas_io.inc", "qas_tma.cuh", "qas_dd.inc"]
+           "qas_io.inc", "qas_tma.cuh", "qas_dd.inc", "qas_hall.cuh", "qas_pipe.cuh", "qas_pipe.inc"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

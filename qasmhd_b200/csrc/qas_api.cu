@@ -22,6 +22,7 @@
 #include "qas_kernels.cuh"
 #include "qas_tma.cuh"
 #include "qas_hall.cuh"
+#include "qas_pipe.cuh"
 
 using namespace qas;
 
@@ -52,6 +53,9 @@ struct AdjState;  // discrete-adjoint run state (qas_adjoint_api.inc)
 static void adj_free(qas_ctx *c);
 struct IoState;  // asynchronous output writer (qas_io.inc)
 static void io_free(qas_ctx *c);
+struct PipeState;  // host round trip with overlapped copies (qas_pipe.inc)
+static void pipe_free(qas_ctx *c);
+static qas_status pipe_set_items(qas_ctx *c, int value);
 
 struct qas_ctx {
   int device = 0;
@@ -109,6 +113,7 @@ struct qas_ctx {
   LrTmaMaps lr_maps[3];
   LrTmaPlan lr_plan[3];
   int lr_grid[3] = {0, 0, 0};
+  PipeState *pipe = nullptr;  // qas_step_host: stage buffers, copy streams, item plan
 };
 
 // ---------------------------------------------------------------------------
@@ -921,6 +926,7 @@ qas_status qas_destroy(qas_ctx *c)
   if (c->stream) cudaStreamSynchronize(c->stream);
   adj_free(c);
   io_free(c);
+  pipe_free(c);
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
   if (c->pool) cudaFree(c->pool);
@@ -1456,6 +1462,7 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
     c->lr_tma = t;
     return QAS_OK;
   }
+  if (option == QAS_OPT_PIPE_ITEMS) return pipe_set_items(c, value);
   return QAS_ERR_INVALID;
 }
 
@@ -1645,3 +1652,4 @@ qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 #include "qas_noalloc.inc"
 #include "qas_io.inc"
 #include "qas_dd.inc"
+#include "qas_pipe.inc"

@@ -1,0 +1,195 @@
+// qas_pipe.cuh -- kernels of the pipelined host round trip (qas_step_host): the cell kernels
+// of one exec_ step restricted to a window of planes along the last axis (rows in 2D, z planes
+// in 3D).  Every kernel calls the same per-cell body as its full-grid counterpart, so a value
+// computed here is bit-identical to the one the full-grid kernel computes at that cell from
+// the same inputs.
+#pragma once
+
+#include "qas_kernels.cuh"
+
+namespace qas {
+
+// Launched with programmatic dependent launch: a kernel may start while the previous one in
+// its stream drains, and waits for its completion (and its memory) before touching anything.
+#define QAS_PDL_WAIT() cudaGridDependencySynchronize()
+
+// planes [lo, hi) of the last axis, padded index
+struct Rows {
+  int lo, hi;
+};
+
+// the eight state arrays of one stage buffer
+struct StatePtrs {
+  double *p[8];
+};
+
+__device__ __forceinline__ bool win_cell(const Geo &g, Rows r, int &i, int &j, int &k)
+{
+  i = blockIdx.x * blockDim.x + threadIdx.x;
+  j = blockIdx.y * blockDim.y + threadIdx.y;
+  k = blockIdx.z * blockDim.z + threadIdx.z;
+  int &h = g.dim == 3 ? k : j;
+  h += r.lo;
+  return i < g.nx && j < g.ny && k < g.nz && h < r.hi;
+}
+
+template <int ODR>
+__global__ void QAS_PRIM_BOUNDS kw_prim(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  prim_body<ODR>(v, i, j, k);
+}
+
+__global__ void kw_dv(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  dv_body(v, i, j, k);
+}
+
+template <int ODR, int A, int PR>
+__global__ void __launch_bounds__(128, QAS_LR_MINB) kw_lr(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  lr_body<ODR, A, PR>(v, i, j, k);
+}
+
+template <int RMN, int A>
+__global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) kw_flux(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  flux_body<RMN, A>(v, i, j, k);
+}
+
+template <int A>
+__global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  flux_body<3, A>(v, i, j, k);
+}
+
+template <int ODR>
+__global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  emf_body<ODR>(v, i, j, k);
+}
+
+// the update cells of k_update (i in [GH, nx-GH], likewise j in 3D) on planes [lo, hi), which
+// lie in [GH, n-GH] (the last face plane of the staggered field included)
+template <int ODR>
+__global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows r, double c0, double c1)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int i = GH + blockIdx.x * blockDim.x + threadIdx.x;
+  const int tj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tk = blockIdx.z * blockDim.z + threadIdx.z;
+  int j, k;
+  if (g.dim == 3) {
+    j = GH + tj;
+    k = r.lo + tk;
+    if (j > g.ny - GH || k >= r.hi) return;
+  } else {
+    j = r.lo + tj;
+    k = 0;
+    if (tk > 0 || j >= r.hi) return;
+  }
+  if (i > g.nx - GH) return;
+  update_body<ODR>(v, i, j, k, c0, c1);
+}
+
+// ghost fill of the cells of planes [lo, hi) that are ghosts along an in-plane axis (x in 2D;
+// x or y in 3D).  Their sources lie in the same plane.
+__global__ void kw_bound_cols(View v, Rows r)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (g.dim == 2) {
+    const long long per = 2 * GH;
+    if (t >= per * (r.hi - r.lo)) return;
+    const int col = (int)(t % per);
+    i = col < GH ? col : g.nx - 2 * GH + col;
+    j = r.lo + (int)(t / per);
+    k = 0;
+  } else {
+    const long long per = (long long)g.nx * g.ny - (long long)(g.nx - 2 * GH) * (g.ny - 2 * GH);
+    if (t >= per * (r.hi - r.lo)) return;
+    Geo g2 = g;
+    g2.dim = 2;
+    int kk;
+    shell_cell(g2, t % per, i, j, kk);
+    k = r.lo + (int)(t / per);
+  }
+  bound_body(v, i, j, k);
+}
+
+// ghost fill of the ghost planes of the last axis ([0, GH) and [n-GH, n), every in-plane cell)
+__global__ void kw_bound_ends(View v)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const long long plane = g.dim == 3 ? (long long)g.nx * g.ny : (long long)g.nx;
+  const int n = g.dim == 3 ? g.nz : g.ny;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * GH * plane) return;
+  const int h = (int)(t / plane);
+  const int hh = h < GH ? h : n - 2 * GH + h;
+  const long long q = t % plane;
+  int i, j, k;
+  if (g.dim == 3) {
+    i = (int)(q % g.nx);
+    j = (int)(q / g.nx);
+    k = hh;
+  } else {
+    i = (int)q;
+    j = hh;
+    k = 0;
+  }
+  bound_body(v, i, j, k);
+}
+
+// planes [lo, hi) of the eight state arrays, src -> dst: field blockIdx.y, two doubles per thread
+// (no stop-flag guard: a finished run carries its state through unchanged)
+__global__ void kw_copy(StatePtrs dst, StatePtrs src, long long off, long long count)
+{
+  QAS_PDL_WAIT();
+  const double *a = src.p[blockIdx.y] + off;
+  double *b = dst.p[blockIdx.y] + off;
+  const long long pairs = count >> 1;
+  const bool aligned = ((((size_t)a) | ((size_t)b)) & 15) == 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pairs;
+       t += (long long)gridDim.x * blockDim.x) {
+    if (aligned)
+      reinterpret_cast<double2 *>(b)[t] = reinterpret_cast<const double2 *>(a)[t];
+    else {
+      b[2 * t] = a[2 * t];
+      b[2 * t + 1] = a[2 * t + 1];
+    }
+  }
+  if ((count & 1) && blockIdx.x == 0 && threadIdx.x == 0) b[count - 1] = a[count - 1];
+}
+
+}  // namespace qas

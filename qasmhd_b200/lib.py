@@ -32,7 +32,7 @@ EXPORTS = (
     "qas_status_str", "qas_abi_version", "qas_last_cuda_error", "qas_create", "qas_destroy",
     "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
-    "qas_run", "qas_run_reset", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
+    "qas_run", "qas_run_reset", "qas_step_host", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
@@ -44,6 +44,7 @@ EXPORTS = (
 )
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
+QAS_OPT_PIPE_ITEMS = 3
 
 
 class QasError(RuntimeError):
@@ -130,6 +131,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_cfl_dt.argtypes = [vp, ctypes.c_double, dp]
     lib.qas_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
     lib.qas_run_reset.argtypes = [vp]
+    lib.qas_step_host.argtypes = [vp, dp, dp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
     lib.qas_dissipate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qas_dsptv.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qas_max_divb.argtypes = [vp, dp]
@@ -349,6 +351,18 @@ class Context:
                     1 if use_graph else 0, float(nu0), float(eta0))
         info = RunInfo()
         _check(self.lib.qas_run(self.h, ctypes.byref(o), ctypes.byref(info)), "qas_run")
+        return info
+
+    def step_host(self, inp: np.ndarray, out: np.ndarray, flg: int = 1, stop_rule: int = 0, cfl: float = 0.4,
+                  dtrec: float = 1.0, nout: int = 1) -> RunInfo:
+        """One exec_ step on host blocks of 8*nd float64 (qas_step_host): upload, step and
+        download with the copies overlapped; out may be inp (pinned memory for the overlap)."""
+        for a in (inp, out):
+            assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.size == 8 * self.nd
+        o = RunOpts(1, int(flg), int(stop_rule), float(cfl), float(dtrec), int(nout), 0, 0.0, 0.0)
+        info = RunInfo()
+        _check(self.lib.qas_step_host(self.h, _dptr(inp), _dptr(out), ctypes.byref(o), ctypes.byref(info)),
+               "qas_step_host")
         return info
 
     def profile(self, nsteps: int, flg: int = 1, cfl: float = 0.4, nu0: float = 0.0, eta0: float = 0.0) -> dict:

@@ -1,0 +1,135 @@
+"""qas_step_host: one exec_ step on host arrays with the copies overlapped by items of planes.
+
+Its contract is the serial composition qas_upload_block + qas_run(one step) +
+qas_download_block: every step's state (interior and ghosts) and loop state (n, tim, dt) must
+be bit-identical to it, over several consecutive steps (setdt every second step), for every
+solver, both boundary kinds of the last axis (periodic: the seam item wraps; open), 2D and 3D,
+any item count, with the output block aliasing the input or not.  Forms the wave does not
+cover (1D, gravity) must give the same bits through the serial path."""
+import numpy as np
+import pytest
+
+from oracle import refcase as R
+from qasmhd_b200 import lib as L
+from qasmhd_b200 import problems as P
+from tests.cases import assert_bitwise
+
+pytestmark = pytest.mark.gpu
+
+
+def _prim(p):
+    p.char_mode = 1
+    return p
+
+
+CASES = {
+    "ot2d_128_hlld": lambda: P.orszag_tang(128),
+    "ot2d_96x160_roe_ctw0": lambda: P.orszag_tang(96, rmn=P.RMN_ROE, ctw=0, nym=160),
+    "kh2d_64x128_mlau_open_y": lambda: P.kelvin_helmholtz(2, 64, nym=128, mach=0.3),
+    "kh2d_80x144_lhlld_odr2": lambda: P.kelvin_helmholtz(2, 80, nym=144, mach=0.5, rmn=P.RMN_LHLLD, odr=2),
+    "ot2d_128_prim": lambda: _prim(P.orszag_tang(128)),
+    "kh3d_16x16x96_mlau": lambda: P.kelvin_helmholtz(3, 16, nzm=96, mach=0.3),
+    "kh3d_24x16x80_lhlld": lambda: P.kelvin_helmholtz(3, 24, nym=16, nzm=80, mach=0.3, rmn=P.RMN_LHLLD),
+    "wave3d_20_open_z_roe": lambda: P.smooth_wave(3, 20, rmn=P.RMN_ROE,
+                                                  dn=((0,) * 8, (0,) * 8, (2, 1, 1, -1, 1, 1, -1, 2))),
+}
+
+
+def _serial(p, nsteps):
+    """The reference composition: upload, one exec_ step, download, per step."""
+    h = np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1).copy()
+    states, infos = [], []
+    with L.Context.from_problem(p) as ctx:
+        for _ in range(nsteps):
+            ctx.upload(h)
+            info = ctx.run(max_steps=1, flg=p.flg, stop_rule=0, cfl=p.cfl, use_graph=False)
+            ctx.download_into(h)
+            states.append(h.copy())
+            infos.append((info.n, info.tim, info.dt, info.steps))
+    return states, infos
+
+
+def _block(p, pinned):
+    """The initial state as a host block of 8*nd float64 (pinned: page-locked by torch)."""
+    a = np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1)
+    if not pinned:
+        return a.copy(), None
+    import torch
+    t = torch.empty((8, p.nd), dtype=torch.float64, pin_memory=True)
+    t.copy_(torch.from_numpy(a))
+    return t.numpy(), t  # keep the tensor alive beside its view
+
+
+def _piped(p, nsteps, items=None, alias=True, pinned=False, replan_at=None):
+    h, keep_h = _block(p, pinned)
+    out, keep_o = (h, None) if alias else _block(p, pinned)
+    states, infos = [], []
+    with L.Context.from_problem(p) as ctx:
+        if items is not None:
+            ctx.set_option(L.QAS_OPT_PIPE_ITEMS, items)
+        for step in range(nsteps):
+            if replan_at is not None and step == replan_at:
+                ctx.set_option(L.QAS_OPT_PIPE_ITEMS, 3)
+            info = ctx.step_host(h, out, flg=p.flg, stop_rule=0, cfl=p.cfl)
+            if not alias:
+                h, out = out, h
+            states.append(h.copy())
+            infos.append((info.n, info.tim, info.dt, info.steps))
+        # the context's device state is the last step's result
+        assert np.array_equal(ctx.download(), h)
+    return states, infos
+
+
+def _compare(a, b, label):
+    (sa, ia), (sb, ib) = a, b
+    for k, (x, y) in enumerate(zip(sa, sb)):
+        assert_bitwise(y, x, f"{label} step {k + 1}")
+    assert ib == ia, (label, ia, ib)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_step_host_matches_serial_composition(case):
+    p = CASES[case]()
+    _compare(_serial(p, 5), _piped(p, 5), case)
+
+
+@pytest.mark.parametrize("items", [1, 2, 3, 5, 16, 64])
+def test_step_host_any_item_count(items):
+    p = P.orszag_tang(256, nym=192)
+    _compare(_serial(p, 4), _piped(p, 4, items=items), f"items={items}")
+
+
+def test_step_host_separate_output_block():
+    p = P.kelvin_helmholtz(3, 16, nzm=64, mach=0.3)
+    _compare(_serial(p, 4), _piped(p, 4, alias=False), "out != in")
+
+
+def test_step_host_matches_oracle(restatement):
+    p = P.orszag_tang(64, nym=96)
+    states, infos = _piped(p, 4)
+    want = restatement.run(p, 4, mode=R.MODE_RUN)
+    assert_bitwise(states[-1].reshape(p.state.shape), want["state"], "step_host vs oracle")
+    assert infos[-1][2] == want["dt"]
+
+
+@pytest.mark.parametrize("case", ["bw1d", "rt2d_gravity"])
+def test_step_host_serial_forms(case):
+    p = {"bw1d": lambda: P.brio_wu(128), "rt2d_gravity": lambda: P.rayleigh_taylor(2, 32, 96)}[case]()
+    _compare(_serial(p, 3), _piped(p, 3), case)
+
+
+@pytest.mark.parametrize("case", ["ot2d_128_hlld", "kh2d_64x128_mlau_open_y", "ot2d_128_prim",
+                                  "kh3d_16x16x96_mlau", "wave3d_20_open_z_roe"])
+def test_step_host_pinned_graph(case):
+    """Pinned blocks take the captured graph (one per setdt parity, replayed every other step)."""
+    pytest.importorskip("torch")
+    p = CASES[case]()
+    _compare(_serial(p, 6), _piped(p, 6, pinned=True), f"{case} pinned")
+
+
+def test_step_host_pinned_graph_rebuilds():
+    """A new block pair (in/out swapped every step) or a new item plan captures a new graph."""
+    pytest.importorskip("torch")
+    p = P.orszag_tang(160, nym=200)
+    _compare(_serial(p, 5), _piped(p, 5, pinned=True, alias=False), "swapped blocks")
+    _compare(_serial(p, 6), _piped(p, 6, pinned=True, replan_at=3), "re-planned")
