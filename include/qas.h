@@ -165,7 +165,9 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * processed in items (QAS_OPT_PIPE_ITEMS), the upload of later items runs beside the first
  * stage of earlier ones and the download of finished items beside the last stage of later
  * ones; pinned host memory is needed for the overlap.  The first such call allocates two
- * stage buffers (16 doubles per cell).  opts->max_steps is ignored (one step). */
+ * stage buffers (16 doubles per cell) and, when they fit, the work arrays of two more stage
+ * lanes (61 doubles per cell each; without them the stages share one stream).
+ * opts->max_steps is ignored (one step). */
 qas_status qas_step_host(qas_ctx *ctx, const double *in, double *out, const qas_run_opts *opts, qas_run_info *info);
 
 /* Visco-resistive update with uniform coefficients: DMHD2D::setdc + the sub-cycled
@@ -248,7 +250,7 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
  * All forms give bit-identical results. */
 #define QAS_OPT_FUSED_SWEEP 1
 #define QAS_OPT_LR_STAGING 2
-#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 8) */
+#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 12) */
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel
