@@ -276,6 +276,30 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
         b.synchronize()
         ms = a.elapsed_time(b) / steps
         prof = ctx.profile(2, flg=1, cfl=prob.cfl)
+        # the host round trip per step (1.18 GB each way): serial phases vs qas_step_host
+        host = torch.empty((8, prob.nd), dtype=torch.float64, pin_memory=True)
+        ctx.download_into(host.numpy())
+        hptr = host.numpy()
+
+        def e2e_ms(fn, n):
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
+            a.record(ext)
+            for _ in range(n):
+                fn()
+            b.record(ext)
+            b.synchronize()
+            return a.elapsed_time(b) / n
+
+        def serial_step():
+            ctx.upload(hptr)
+            ctx.run(max_steps=1, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=False)
+            ctx.download_into(hptr)
+
+        ms_serial = e2e_ms(serial_step, 3)
+        ms_host = e2e_ms(lambda: ctx.step_host(hptr, hptr, flg=1, stop_rule=0, cfl=prob.cfl), 3)
+        del host
     gpu = prob.interior_cells / (ms * 1e-3) / 1e6
     cpu = cpu_baseline(prob, steps=cpu_steps) if cpu_steps > 0 else None
     cpu3 = cpu_baseline_o3(prob, steps=cpu_steps) if cpu_steps > 0 else None
@@ -283,6 +307,11 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
            "unit": "Mcell-updates/s", "ms_per_step": ms, "steps": steps,
            "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
            "cpu_baseline": cpu, "cpu_baseline_o3": cpu3,
+           "e2e": {"value": prob.interior_cells / (ms_host * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+                   "ms_per_step": ms_host, "h2d_bytes_per_step": 64 * prob.nd, "d2h_bytes_per_step": 64 * prob.nd,
+                   "api": "qas_step_host"},
+           "e2e_serial": {"value": prob.interior_cells / (ms_serial * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+                          "ms_per_step": ms_serial},
            "step_roofline": {"achieved": ALG_BYTES_PER_CELL_UPDATE * prob.interior_cells / (ms * 1e-3) / 1e9,
                              "unit": "GB/s", "basis": "512 algorithmic B per cell-update"}}
     if cpu:
