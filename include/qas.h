@@ -160,7 +160,7 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * + qas_run(opts, one step) + qas_download_block(out) -- the drop-in for a call of ideal()
  * (mhd2d_solve.cpp:3-400 via exec_, mhd2d_class.cpp:35-61) on the caller's val[] arrays, which
  * the reference updates in place (in == out is allowed).  In and out are blocks of 8*nd
- * doubles in the qas_upload_block layout.  From the second step of a run on, 2D and 3D contexts
+ * doubles in the qas_upload_block layout, in host memory or in device memory.  From the second step of a run on, 2D and 3D contexts
  * without Hall, gravity or dissipation overlap the copies with the kernels: the last axis is
  * processed in items (QAS_OPT_PIPE_ITEMS), the upload of later items runs beside the first
  * stage of earlier ones and the download of finished items beside the last stage of later
