@@ -13,8 +13,31 @@ namespace qas {
 struct BMap {
   int nblocks;
   const int2 *blk;   // (instance, local block index) per block
-  const int4 *grid;  // per instance: launch grid in blocks (x, y, z)
+  const int4 *grid;  // per instance: launch grid in blocks (x, y, z, 0), or the thread extent
+                     // (x, y, z, -1) of a linear map
 };
+
+// the thread's index in its instance's launch extent.  Tiled: block lb is tile (bx, by, bz) of
+// the instance's grid.  Linear: block lb covers threads [lb*T, (lb+1)*T) of the extent in x-fastest
+// order, so no thread idles at the end of a row whatever the instance's size; threads past the
+// extent get an index that fails every range test.
+__device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, int &tk)
+{
+  if (gd.w < 0) {
+    const int nt = blockDim.x * blockDim.y * blockDim.z;
+    const int lin = lb * nt + (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+    const int r = lin / gd.x;
+    ti = lin - r * gd.x;
+    tj = r % gd.y;
+    tk = r / gd.y;
+    if (tk >= gd.z) ti = tj = tk = 1 << 29;
+  } else {
+    const int bx = lb % gd.x, by = (lb / gd.x) % gd.y, bz = lb / (gd.x * gd.y);
+    ti = bx * blockDim.x + threadIdx.x;
+    tj = by * blockDim.y + threadIdx.y;
+    tk = bz * blockDim.z + threadIdx.z;
+  }
+}
 
 #define QAS_BATCH_BLOCKS(map)                                                         \
   for (int b_ = blockIdx.x; b_ < (map).nblocks; b_ += gridDim.x) {                    \
@@ -22,10 +45,8 @@ struct BMap {
     const View &v = views[bi_.x];                                                     \
     if (v.ctl->done) continue;                                                        \
     const int4 gd_ = (map).grid[bi_.x];                                               \
-    const int bx_ = bi_.y % gd_.x, by_ = (bi_.y / gd_.x) % gd_.y, bz_ = bi_.y / (gd_.x * gd_.y); \
-    const int ti = bx_ * blockDim.x + threadIdx.x;                                    \
-    const int tj = by_ * blockDim.y + threadIdx.y;                                    \
-    const int tk = bz_ * blockDim.z + threadIdx.z;
+    int ti, tj, tk;                                                                   \
+    batch_thread(gd_, bi_.y, ti, tj, tk);
 
 #define QAS_BATCH_END }
 
@@ -46,13 +67,15 @@ __global__ void kb_dv(const View *__restrict__ views, BMap map)
   QAS_BATCH_END
 }
 
-template <int ODR, int A>
+// PR: the face-value form of every instance (0 characteristic, 1 primitive) or -1 (mixed: each
+// instance's View decides)
+template <int ODR, int A, int PR>
 __global__ void __launch_bounds__(128, QAS_LR_MINB) kb_lr(const View *__restrict__ views, BMap map)
 {
   QAS_BATCH_BLOCKS(map)
   if (QAS_BATCH_CELL_OK) {
     const int pos = A == 0 ? ti : (A == 1 ? tj : tk);
-    if (pos >= 2 && pos < v.g.n[A] - 2) lr_body<ODR, A>(v, ti, tj, tk);
+    if (pos >= 2 && pos < v.g.n[A] - 2) lr_body<ODR, A, PR>(v, ti, tj, tk);
   }
   QAS_BATCH_END
 }
