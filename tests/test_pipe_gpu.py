@@ -133,3 +133,32 @@ def test_step_host_pinned_graph_rebuilds():
     p = P.orszag_tang(160, nym=200)
     _compare(_serial(p, 5), _piped(p, 5, pinned=True, alias=False), "swapped blocks")
     _compare(_serial(p, 6), _piped(p, 6, pinned=True, replan_at=3), "re-planned")
+
+
+def test_step_host_stop_rule_reached():
+    """exec_'s time limit (tmax = dtrec * nout) reached after three steps: later calls take no
+    step and hand back the input, as qas_run does."""
+    p = P.orszag_tang(128)
+    with L.Context.from_problem(p) as c0:
+        c0.upload(p.state)
+        tmax = 2.5 * c0.run(max_steps=1, flg=1, stop_rule=0, cfl=p.cfl).dt
+    h1 = np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1).copy()
+    h2 = h1.copy()
+    with L.Context.from_problem(p) as a, L.Context.from_problem(p) as b:
+        for k in range(6):
+            a.upload(h1)
+            ia = a.run(max_steps=1, flg=1, stop_rule=1, cfl=p.cfl, dtrec=tmax, nout=1, use_graph=False)
+            a.download_into(h1)
+            ib = b.step_host(h2, h2, flg=1, stop_rule=1, cfl=p.cfl, dtrec=tmax, nout=1)
+            assert_bitwise(h2, h1, f"call {k + 1}")
+            assert (ib.steps, ib.n, ib.tim, ib.dt) == (ia.steps, ia.n, ia.tim, ia.dt), k
+        assert ia.steps == 0 and ia.n < 6
+
+
+def test_pipe_items_option_range():
+    p = P.orszag_tang(64)
+    with L.Context.from_problem(p) as ctx:
+        for bad in (0, -1, 65):
+            with pytest.raises(L.QasError):
+                ctx.set_option(L.QAS_OPT_PIPE_ITEMS, bad)
+        ctx.set_option(L.QAS_OPT_PIPE_ITEMS, 64)
