@@ -43,6 +43,24 @@ __global__ void QAS_PRIM_BOUNDS kw_prim(View v, Rows r)
   prim_body<ODR>(v, i, j, k);
 }
 
+// the primitives on planes pr and the copy of the eight state arrays v.u -> dst on planes cp, one
+// launch over rows r (their union); the copy ignores the stop flag (a finished run carries its
+// state through)
+template <int ODR>
+__global__ void QAS_PRIM_BOUNDS kw_prim_copy(View v, Rows r, Rows pr, Rows cp, StatePtrs dst)
+{
+  QAS_PDL_WAIT();
+  int i, j, k;
+  if (!win_cell(v.g, r, i, j, k)) return;
+  const int h = v.g.dim == 3 ? k : j;
+  if (h >= cp.lo && h < cp.hi) {
+    const long long c = cidx(v.g, i, j, k);
+#pragma unroll
+    for (int m = 0; m < 8; m++) dst.p[m][c] = v.u[m][c];
+  }
+  if (!v.ctl->done && h >= pr.lo && h < pr.hi) prim_body<ODR>(v, i, j, k);
+}
+
 __global__ void kw_dv(View v, Rows r)
 {
   QAS_PDL_WAIT();
@@ -169,27 +187,6 @@ __global__ void kw_bound_ends(View v)
     k = 0;
   }
   bound_body(v, i, j, k);
-}
-
-// planes [lo, hi) of the eight state arrays, src -> dst: field blockIdx.y, two doubles per thread
-// (no stop-flag guard: a finished run carries its state through unchanged)
-__global__ void kw_copy(StatePtrs dst, StatePtrs src, long long off, long long count)
-{
-  QAS_PDL_WAIT();
-  const double *a = src.p[blockIdx.y] + off;
-  double *b = dst.p[blockIdx.y] + off;
-  const long long pairs = count >> 1;
-  const bool aligned = ((((size_t)a) | ((size_t)b)) & 15) == 0;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < pairs;
-       t += (long long)gridDim.x * blockDim.x) {
-    if (aligned)
-      reinterpret_cast<double2 *>(b)[t] = reinterpret_cast<const double2 *>(a)[t];
-    else {
-      b[2 * t] = a[2 * t];
-      b[2 * t + 1] = a[2 * t + 1];
-    }
-  }
-  if ((count & 1) && blockIdx.x == 0 && threadIdx.x == 0) b[count - 1] = a[count - 1];
 }
 
 }  // namespace qas
