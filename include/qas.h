@@ -165,8 +165,9 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * processed in items (QAS_OPT_PIPE_ITEMS), the upload of later items runs beside the first
  * stage of earlier ones and the download of finished items beside the last stage of later
  * ones; pinned host memory is needed for the overlap.  The first such call allocates two
- * stage buffers (16 doubles per cell) and, when they fit, the work arrays of two more stage
- * lanes (61 doubles per cell each; without them the stages share one stream).
+ * stage buffers (16 doubles per cell; when they do not fit, every call takes the serial
+ * phases) and, when they fit, the work arrays of two more stage lanes (61 doubles per cell
+ * each; without them the stages share one stream).
  * opts->max_steps is ignored (one step). */
 qas_status qas_step_host(qas_ctx *ctx, const double *in, double *out, const qas_run_opts *opts, qas_run_info *info);
 
