@@ -40,7 +40,11 @@ K_LR_FP64_INSTR_PER_CELL = 1054.0
 K_LR_FP64_FLOPS_PER_CELL = 1262.0
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_lr launch (y direction) on the
 # same workload (profiles/k_lr_ot2d_1024.md)
-K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.70e6 + 92.25e6}
+K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.70e6 + 92.25e6,
+                           # KH 128^3 capture (x faces, 136^3 padded cells: 200.12 + 314.29 MB),
+                           # scaled by padded cells to 264^3 (traffic per cell is size-independent:
+                           # every array is streamed once, the 126 MB L2 holds no full array)
+                           "kh3d_256": (200.12e6 + 314.29e6) * (264 / 136) ** 3}
 
 
 def parse():
