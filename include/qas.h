@@ -251,7 +251,7 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
  * All forms give bit-identical results. */
 #define QAS_OPT_FUSED_SWEEP 1
 #define QAS_OPT_LR_STAGING 2
-#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 16 in 2D, 8 in 3D) */
+#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 16) */
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

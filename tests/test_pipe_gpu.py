@@ -6,6 +6,8 @@ be bit-identical to it, over several consecutive steps (setdt every second step)
 solver, both boundary kinds of the last axis (periodic: the seam item wraps; open), 2D and 3D,
 any item count, with the output block aliasing the input or not.  Forms the wave does not
 cover (1D, gravity) must give the same bits through the serial path."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -162,3 +164,20 @@ def test_pipe_items_option_range():
             with pytest.raises(L.QasError):
                 ctx.set_option(L.QAS_OPT_PIPE_ITEMS, bad)
         ctx.set_option(L.QAS_OPT_PIPE_ITEMS, 64)
+
+
+def test_step_host_rejects_null_arguments():
+    p = P.orszag_tang(64)
+    h = np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1).copy()
+    hp = h.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    null = ctypes.POINTER(ctypes.c_double)()
+    with L.Context.from_problem(p) as ctx:
+        o = L.RunOpts(1, 1, 0, float(p.cfl), 1.0, 1, 0, 0.0, 0.0)
+        info = L.RunInfo()
+        lib = ctx.lib
+        assert lib.qas_step_host(ctx.h, null, hp, ctypes.byref(o), ctypes.byref(info)) == L.QAS_ERR_INVALID
+        assert lib.qas_step_host(ctx.h, hp, null, ctypes.byref(o), ctypes.byref(info)) == L.QAS_ERR_INVALID
+        assert lib.qas_step_host(ctx.h, hp, hp, None, ctypes.byref(info)) == L.QAS_ERR_INVALID
+        bad = L.RunOpts(1, 1, 3, float(p.cfl), 1.0, 1, 0, 0.0, 0.0)  # no stop rule 3
+        assert lib.qas_step_host(ctx.h, hp, hp, ctypes.byref(bad), ctypes.byref(info)) == L.QAS_ERR_INVALID
+        ctx.step_host(h, h, flg=1, stop_rule=0, cfl=p.cfl)  # the context is still usable
