@@ -162,7 +162,7 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * the reference updates in place (in == out is allowed).  In and out are blocks of 8*nd
  * doubles in the qas_upload_block layout, in host memory or in device memory.  From the second step of a run on, 2D and 3D contexts
  * without Hall, gravity or dissipation overlap the copies with the kernels: the last axis is
- * processed in items (QAS_OPT_PIPE_ITEMS), the upload of later items runs beside the first
+ * processed in windows of planes (QAS_OPT_PIPE_ITEMS), the upload of later ones runs beside the first
  * stage of earlier ones and the download of finished items beside the last stage of later
  * ones; pinned host memory is needed for the overlap.  The first such call allocates two
  * stage buffers (16 doubles per cell; when they do not fit, every call takes the serial
@@ -251,7 +251,7 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
  * All forms give bit-identical results. */
 #define QAS_OPT_FUSED_SWEEP 1
 #define QAS_OPT_LR_STAGING 2
-#define QAS_OPT_PIPE_ITEMS 3 /* items of qas_step_host's wave along the last axis, 1..64 (default 16) */
+#define QAS_OPT_PIPE_ITEMS 3 /* windows of planes of qas_step_host's wave, 1..64 (default 32) */
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

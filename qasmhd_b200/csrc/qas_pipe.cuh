@@ -23,45 +23,54 @@ struct StatePtrs {
   double *p[8];
 };
 
-__device__ __forceinline__ bool win_cell(const Geo &g, Rows r, int &i, int &j, int &k)
+// up to two disjoint plane ranges handled by one launch (b empty for one range); the
+// launch's last grid axis counts the planes of a, then those of b
+struct Rows2 {
+  Rows a, b;
+};
+
+__device__ __forceinline__ int rows_len(Rows r) { return r.hi > r.lo ? r.hi - r.lo : 0; }
+__device__ __forceinline__ bool rows_has(Rows r, int h) { return h >= r.lo && h < r.hi; }
+__device__ __forceinline__ bool rows2_has(const Rows2 &r, int h) { return rows_has(r.a, h) || rows_has(r.b, h); }
+
+// the t-th plane of r, or -1 past its end
+__device__ __forceinline__ int rows2_plane(const Rows2 &r, int t)
+{
+  const int na = rows_len(r.a);
+  if (t < na) return r.a.lo + t;
+  t -= na;
+  return t < rows_len(r.b) ? r.b.lo + t : -1;
+}
+
+__device__ __forceinline__ bool win_cell(const Geo &g, const Rows2 &r, int &i, int &j, int &k)
 {
   i = blockIdx.x * blockDim.x + threadIdx.x;
   j = blockIdx.y * blockDim.y + threadIdx.y;
   k = blockIdx.z * blockDim.z + threadIdx.z;
   int &h = g.dim == 3 ? k : j;
-  h += r.lo;
-  return i < g.nx && j < g.ny && k < g.nz && h < r.hi;
-}
-
-template <int ODR>
-__global__ void QAS_PRIM_BOUNDS kw_prim(View v, Rows r)
-{
-  QAS_PDL_WAIT();
-  if (v.ctl->done) return;
-  int i, j, k;
-  if (!win_cell(v.g, r, i, j, k)) return;
-  prim_body<ODR>(v, i, j, k);
+  h = rows2_plane(r, h);
+  return h >= 0 && i < g.nx && j < g.ny && k < g.nz;
 }
 
 // the primitives on planes pr and the copy of the eight state arrays v.u -> dst on planes cp, one
 // launch over rows r (their union); the copy ignores the stop flag (a finished run carries its
 // state through)
 template <int ODR>
-__global__ void QAS_PRIM_BOUNDS kw_prim_copy(View v, Rows r, Rows pr, Rows cp, StatePtrs dst)
+__global__ void QAS_PRIM_BOUNDS kw_prim_copy(View v, Rows2 r, Rows2 pr, Rows2 cp, StatePtrs dst)
 {
   QAS_PDL_WAIT();
   int i, j, k;
   if (!win_cell(v.g, r, i, j, k)) return;
   const int h = v.g.dim == 3 ? k : j;
-  if (h >= cp.lo && h < cp.hi) {
+  if (rows2_has(cp, h)) {
     const long long c = cidx(v.g, i, j, k);
 #pragma unroll
     for (int m = 0; m < 8; m++) dst.p[m][c] = v.u[m][c];
   }
-  if (!v.ctl->done && h >= pr.lo && h < pr.hi) prim_body<ODR>(v, i, j, k);
+  if (!v.ctl->done && rows2_has(pr, h)) prim_body<ODR>(v, i, j, k);
 }
 
-__global__ void kw_dv(View v, Rows r)
+__global__ void kw_dv(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -71,7 +80,7 @@ __global__ void kw_dv(View v, Rows r)
 }
 
 template <int ODR, int A, int PR>
-__global__ void __launch_bounds__(128, QAS_LR_MINB) kw_lr(View v, Rows r)
+__global__ void __launch_bounds__(128, QAS_LR_MINB) kw_lr(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -81,7 +90,7 @@ __global__ void __launch_bounds__(128, QAS_LR_MINB) kw_lr(View v, Rows r)
 }
 
 template <int RMN, int A>
-__global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) kw_flux(View v, Rows r)
+__global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) kw_flux(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -91,7 +100,7 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MINB_OF(RMN)) kw_flux(View v, Ro
 }
 
 template <int A>
-__global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, Rows r)
+__global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -101,7 +110,7 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, 
 }
 
 template <int ODR>
-__global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows r)
+__global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -113,7 +122,7 @@ __global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows r)
 // the update cells of k_update (i in [GH, nx-GH], likewise j in 3D) on planes [lo, hi), which
 // lie in [GH, n-GH] (the last face plane of the staggered field included)
 template <int ODR>
-__global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows r, double c0, double c1)
+__global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows2 r, double c0, double c1)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -124,12 +133,12 @@ __global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows r, double c0, double c1
   int j, k;
   if (g.dim == 3) {
     j = GH + tj;
-    k = r.lo + tk;
-    if (j > g.ny - GH || k >= r.hi) return;
+    k = rows2_plane(r, tk);
+    if (j > g.ny - GH || k < 0) return;
   } else {
-    j = r.lo + tj;
+    j = rows2_plane(r, tj);
     k = 0;
-    if (tk > 0 || j >= r.hi) return;
+    if (tk > 0 || j < 0) return;
   }
   if (i > g.nx - GH) return;
   update_body<ODR>(v, i, j, k, c0, c1);
@@ -137,28 +146,29 @@ __global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows r, double c0, double c1
 
 // ghost fill of the cells of planes [lo, hi) that are ghosts along an in-plane axis (x in 2D;
 // x or y in 3D).  Their sources lie in the same plane.
-__global__ void kw_bound_cols(View v, Rows r)
+__global__ void kw_bound_cols(View v, Rows2 r)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
   const Geo &g = v.g;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int planes = rows_len(r.a) + rows_len(r.b);
   int i, j, k;
   if (g.dim == 2) {
     const long long per = 2 * GH;
-    if (t >= per * (r.hi - r.lo)) return;
+    if (t >= per * planes) return;
     const int col = (int)(t % per);
     i = col < GH ? col : g.nx - 2 * GH + col;
-    j = r.lo + (int)(t / per);
+    j = rows2_plane(r, (int)(t / per));
     k = 0;
   } else {
     const long long per = (long long)g.nx * g.ny - (long long)(g.nx - 2 * GH) * (g.ny - 2 * GH);
-    if (t >= per * (r.hi - r.lo)) return;
+    if (t >= per * planes) return;
     Geo g2 = g;
     g2.dim = 2;
     int kk;
     shell_cell(g2, t % per, i, j, kk);
-    k = r.lo + (int)(t / per);
+    k = rows2_plane(r, (int)(t / per));
   }
   bound_body(v, i, j, k);
 }
