@@ -252,6 +252,8 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
 #define QAS_OPT_FUSED_SWEEP 1
 #define QAS_OPT_LR_STAGING 2
 #define QAS_OPT_PIPE_ITEMS 3 /* windows of planes of qas_step_host's wave, 1..64 (default 32) */
+#define QAS_OPT_PIPE_LANES 4 /* streams of qas_step_host's stages, 1..3 (default 3 when their work arrays
+                                fit); set before the first qas_step_host of the context */
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

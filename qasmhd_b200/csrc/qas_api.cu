@@ -56,6 +56,7 @@ static void io_free(qas_ctx *c);
 struct PipeState;  // host round trip with overlapped copies (qas_pipe.inc)
 static void pipe_free(qas_ctx *c);
 static qas_status pipe_set_items(qas_ctx *c, int value);
+static qas_status pipe_set_lanes(qas_ctx *c, int value);
 
 struct qas_ctx {
   int device = 0;
@@ -1463,6 +1464,7 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
     return QAS_OK;
   }
   if (option == QAS_OPT_PIPE_ITEMS) return pipe_set_items(c, value);
+  if (option == QAS_OPT_PIPE_LANES) return pipe_set_lanes(c, value);
   return QAS_ERR_INVALID;
 }
 

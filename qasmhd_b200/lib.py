@@ -45,6 +45,7 @@ EXPORTS = (
 QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
 QAS_OPT_PIPE_ITEMS = 3
+QAS_OPT_PIPE_LANES = 4
 
 
 class QasError(RuntimeError):

@@ -62,11 +62,13 @@ def _block(p, pinned):
     return t.numpy(), t  # keep the tensor alive beside its view
 
 
-def _piped(p, nsteps, items=None, alias=True, pinned=False, replan_at=None):
+def _piped(p, nsteps, items=None, alias=True, pinned=False, replan_at=None, lanes=None):
     h, keep_h = _block(p, pinned)
     out, keep_o = (h, None) if alias else _block(p, pinned)
     states, infos = [], []
     with L.Context.from_problem(p) as ctx:
+        if lanes is not None:
+            ctx.set_option(L.QAS_OPT_PIPE_LANES, lanes)
         if items is not None:
             ctx.set_option(L.QAS_OPT_PIPE_ITEMS, items)
         for step in range(nsteps):
@@ -181,3 +183,27 @@ def test_step_host_rejects_null_arguments():
         bad = L.RunOpts(1, 1, 3, float(p.cfl), 1.0, 1, 0, 0.0, 0.0)  # no stop rule 3
         assert lib.qas_step_host(ctx.h, hp, hp, ctypes.byref(bad), ctypes.byref(info)) == L.QAS_ERR_INVALID
         ctx.step_host(h, h, flg=1, stop_rule=0, cfl=p.cfl)  # the context is still usable
+
+
+@pytest.mark.parametrize("lanes", [1, 2])
+@pytest.mark.parametrize("case", ["ot2d_128_hlld", "kh3d_16x16x96_mlau"])
+def test_step_host_fewer_lanes(case, lanes):
+    """The stages on fewer streams (what a context gets when the extra work arrays do not fit):
+    one lane keeps every intermediate's halo; bit-identical all the same."""
+    p = CASES[case]()
+    _compare(_serial(p, 5), _piped(p, 5, lanes=lanes, items=12), f"{case} lanes={lanes}")
+    _compare(_serial(p, 4), _piped(p, 4, lanes=lanes, pinned=True), f"{case} lanes={lanes} pinned")
+
+
+def test_pipe_lanes_option_fixed_after_first_use():
+    p = P.orszag_tang(64)
+    h = np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1).copy()
+    with L.Context.from_problem(p) as ctx:
+        for bad in (0, 4):
+            with pytest.raises(L.QasError):
+                ctx.set_option(L.QAS_OPT_PIPE_LANES, bad)
+        ctx.set_option(L.QAS_OPT_PIPE_LANES, 2)
+        for _ in range(2):
+            ctx.step_host(h, h, flg=1, stop_rule=0, cfl=p.cfl)
+        with pytest.raises(L.QasError):
+            ctx.set_option(L.QAS_OPT_PIPE_LANES, 3)
