@@ -207,3 +207,23 @@ def test_pipe_lanes_option_fixed_after_first_use():
             ctx.step_host(h, h, flg=1, stop_rule=0, cfl=p.cfl)
         with pytest.raises(L.QasError):
             ctx.set_option(L.QAS_OPT_PIPE_LANES, 3)
+
+
+def test_step_host_device_blocks():
+    """In and out may be device memory (e.g. torch CUDA tensors): same bits as the serial
+    composition on host arrays."""
+    torch = pytest.importorskip("torch")
+    p = P.kelvin_helmholtz(2, 64, nym=128, mach=0.3)
+    want_states, want_infos = _serial(p, 4)
+    d = torch.from_numpy(np.ascontiguousarray(p.state, dtype=np.float64).reshape(8, -1).copy()).cuda()
+    dp = ctypes.cast(d.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    infos = []
+    with L.Context.from_problem(p) as ctx:
+        o = L.RunOpts(1, int(p.flg), 0, float(p.cfl), 1.0, 1, 0, 0.0, 0.0)
+        for k in range(4):
+            info = L.RunInfo()
+            assert ctx.lib.qas_step_host(ctx.h, dp, dp, ctypes.byref(o), ctypes.byref(info)) == 0
+            torch.cuda.synchronize()
+            assert_bitwise(d.cpu().numpy(), want_states[k], f"device blocks step {k + 1}")
+            infos.append((info.n, info.tim, info.dt, info.steps))
+    assert infos == want_infos
