@@ -170,6 +170,16 @@ qas_status qas_run_reset(qas_ctx *ctx);
  * each; without them the stages share one stream).
  * opts->max_steps is ignored (one step). */
 qas_status qas_step_host(qas_ctx *ctx, const double *in, double *out, const qas_run_opts *opts, qas_run_info *info);
+/* The plan of qas_step_host's wave along a last axis of `planes` padded planes (host only, no
+ * GPU): `windows` as QAS_OPT_PIPE_ITEMS (0: the default), own_lanes = 1 for the ranges used when
+ * every stage has a stream of its own (each plane computed once), 0 for the shared-stream ranges
+ * (every item over its full halo).  *nitems items and the issue *lag; with out != NULL (room for
+ * max_items items), QAS_PIPE_ITEM_INTS ints per item: nseg, ends (holds the ghost planes), then
+ * for each of two segments nine [lo, hi) plane ranges: copied, updated, ghost-filled, primitives,
+ * shock detector, in-plane face states and fluxes, last-axis face states (cells), last-axis
+ * fluxes (faces), EMFs (empty ranges for a missing segment). */
+#define QAS_PIPE_ITEM_INTS 38
+qas_status qas_pipe_plan(int planes, int windows, int own_lanes, int *out, int max_items, int *nitems, int *lag);
 
 /* Visco-resistive update with uniform coefficients: DMHD2D::setdc + the sub-cycled
  * dsptv of DMHD2D::exec_ (2D/SERIAL/MRX/dmhd2d_class.cpp:19-26, dmhd2d_solve.cpp:3-151),

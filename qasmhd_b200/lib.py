@@ -32,7 +32,7 @@ EXPORTS = (
     "qas_status_str", "qas_abi_version", "qas_last_cuda_error", "qas_create", "qas_destroy",
     "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
-    "qas_run", "qas_run_reset", "qas_step_host", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
+    "qas_run", "qas_run_reset", "qas_step_host", "qas_pipe_plan", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
@@ -133,6 +133,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_run.argtypes = [vp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
     lib.qas_run_reset.argtypes = [vp]
     lib.qas_step_host.argtypes = [vp, dp, dp, ctypes.POINTER(RunOpts), ctypes.POINTER(RunInfo)]
+    ipp = ctypes.POINTER(ctypes.c_int)
+    lib.qas_pipe_plan.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ipp, ctypes.c_int, ipp, ipp]
     lib.qas_dissipate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qas_dsptv.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qas_max_divb.argtypes = [vp, dp]
@@ -480,6 +482,31 @@ def bc_map(prob, group: int, field: int, axis: int):
     _check(lib.qas_bc_map(ctypes.byref(g), ctypes.byref(b), group, field, axis,
                           src.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(fac), n), "qas_bc_map")
     return src, fac
+
+
+PIPE_ITEM_INTS = 38
+PIPE_RANGE_NAMES = ("seg", "upd", "bnd", "prim", "dv", "fin", "lax", "fax", "emf")
+
+
+def pipe_plan(planes: int, windows: int = 0, own_lanes: bool = True):
+    """qas_step_host's wave along a last axis of `planes` padded planes (host only): the items,
+    each {"nseg", "ends", name: [(lo, hi), (lo, hi)]} for the ranges of PIPE_RANGE_NAMES, and the
+    issue lag."""
+    lib = load()
+    n, lag = ctypes.c_int(), ctypes.c_int()
+    _check(lib.qas_pipe_plan(int(planes), int(windows), int(bool(own_lanes)), None, 0, ctypes.byref(n),
+                             ctypes.byref(lag)), "qas_pipe_plan")
+    buf = (ctypes.c_int * (PIPE_ITEM_INTS * n.value))()
+    _check(lib.qas_pipe_plan(int(planes), int(windows), int(bool(own_lanes)), buf, n.value, ctypes.byref(n),
+                             ctypes.byref(lag)), "qas_pipe_plan")
+    items = []
+    for q in range(n.value):
+        rec = buf[q * PIPE_ITEM_INTS:(q + 1) * PIPE_ITEM_INTS]
+        it = {"nseg": rec[0], "ends": bool(rec[1])}
+        for k, name in enumerate(PIPE_RANGE_NAMES):
+            it[name] = [(rec[2 + 18 * sg + 2 * k], rec[3 + 18 * sg + 2 * k]) for sg in range(2)]
+        items.append(it)
+    return items, lag.value
 
 
 def dd_plan(prob, nparts: int):
