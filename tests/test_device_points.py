@@ -1,0 +1,80 @@
+"""The device point functions of the step against the reference's own, bit for bit, on the CPU.
+
+qas_device.cuh is host+device code, so a host build of it (tests/native/device_points.cpp,
+g++ without FP contraction: the library is built with --fmad=false and IEEE division and
+square root) is compared with the known-answer vectors of the reference's point functions
+(tests/golden/kat_*.npz, from common/mhd_flux.c, common/common_interp.c, common/mhd_func.c
+built from source): the four Riemann solvers, the linear and nonlinear face interpolations the
+schemes use, the characteristic face states of mhd_lrstate at every order -- the per-field
+form and the grouped-stencil form the kernels run -- and the CUCT weight."""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.cases import assert_bitwise
+from tests.golden import make_golden as G
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+D = ctypes.POINTER(ctypes.c_double)
+
+
+@pytest.fixture(scope="module")
+def dev(tmp_path_factory):
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    out = str(tmp_path_factory.mktemp("pts") / "device_points.so")
+    subprocess.run([cxx, "-O2", "-ffp-contract=off", "-std=c++17", "-shared", "-fPIC",
+                    "-I", os.path.join(ROOT, "qasmhd_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "native", "device_points.cpp"), "-o", out], check=True)
+    lib = ctypes.CDLL(out)
+    lib.t_cuct.restype = ctypes.c_double
+    lib.t_cuct.argtypes = [D]
+    for f in (lib.t_flux, lib.t_lin, lib.t_nl):
+        f.argtypes = [ctypes.c_int, D, D]
+    lib.t_face_states.argtypes = [ctypes.c_int, ctypes.c_int, D, D]
+    return lib
+
+
+def _run(fn, inp, nout, *lead):
+    out = np.zeros((inp.shape[0], nout))
+    for c in range(inp.shape[0]):
+        a = np.ascontiguousarray(inp[c])
+        fn(*lead, a.ctypes.data_as(D), out[c].ctypes.data_as(D))
+    return out
+
+
+@pytest.mark.parametrize("rmn", [0, 1, 2, 3])
+def test_riemann_solvers(dev, rmn):
+    inp = G.kat_inputs("flux")
+    gold = np.load(os.path.join(GOLD, "kat_flux.npz"))[f"f{rmn}"]
+    assert_bitwise(_run(dev.t_flux, inp, 7, rmn), gold, f"riemann {rmn}")
+
+
+@pytest.mark.parametrize("kat,form,odr", [(10, "lin", 1), (11, "lin", 2), (12, "lin", 3), (13, "lin", 4),
+                                          (10, "nl", 1), (14, "nl", 2), (15, "nl", 3), (16, "nl", 4)])
+def test_face_interpolations(dev, kat, form, odr):
+    inp = G.kat_inputs("interp")
+    gold = np.load(os.path.join(GOLD, "kat_interp.npz"))[f"f{kat}"]
+    fn = dev.t_lin if form == "lin" else dev.t_nl
+    assert_bitwise(_run(fn, inp, 2, odr), gold, f"{form} order {odr}")
+
+
+@pytest.mark.parametrize("grouped", [0, 1])
+@pytest.mark.parametrize("odr", [1, 2, 3, 4])
+def test_characteristic_face_states(dev, odr, grouped):
+    inp = G.kat_inputs("lrstate")
+    gold = np.load(os.path.join(GOLD, "kat_lrstate.npz"))[f"f{19 + odr}"]
+    assert_bitwise(_run(dev.t_face_states, inp, 14, odr, grouped), gold, f"mhd_lrstate order {odr} grouped {grouped}")
+
+
+def test_cuct_weight(dev):
+    inp = G.kat_inputs("cuct")
+    gold = np.load(os.path.join(GOLD, "kat_cuct.npz"))["f30"]
+    got = np.array([[dev.t_cuct(np.ascontiguousarray(r).ctypes.data_as(D))] for r in inp])
+    assert_bitwise(got, gold, "cuct weight")
