@@ -1975,11 +1975,12 @@ int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out
       riemann(func)(&a[0], &a[7], a[14], a[15], &a[16], o);
     } else if (func >= 10 && func <= 19) {
       lrs[func - 10](&a[2], &o[0], &o[1]);
-    } else if (func >= 20 && func <= 23) {
+    } else if (func >= 20 && func <= 27) {  /* 24..27: with the primitive reconstruction */
       double q[7][5];
+      const int prim = func >= 24;
       for (int v = 0; v < 7; v++)
         for (int m = 0; m < 5; m++) q[v][m] = a[5 * v + m];
-      face_states(q, a[35], a[36], nl_interp(func - 19), &o[0], &o[7], 0);
+      face_states(q, a[35], a[36], nl_interp(func - (prim ? 23 : 19)), &o[0], &o[7], prim);
     } else if (func == 30) {
       o[0] = cuct_weight(&a[3], &a[7], &a[11], &a[15], &a[19], 1, 2);
     } else if (func == 31) {

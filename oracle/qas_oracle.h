@@ -65,7 +65,9 @@ int qo_dissipate(const qo_grid *g, double *u, double dt, double nu0, double eta0
 int qo_hall(const qo_grid *g, double *u, double dt, double di, double vphix);
 double qo_haldt(const qo_grid *g, const double *u, double cfl, double di, double vphix);
 
-/* Point-function known answers; same function ids and layouts as oracle/ref_harness/ref_kat.cpp. */
+/* Point-function known answers; same function ids and layouts as oracle/ref_harness/ref_kat.cpp,
+ * plus 24..27: mhd_lrstate at ODR 1..4 with the primitive reconstruction mhd_reconst (the ids
+ * 20..23 of the harness built against it, oracle/_ref/ref_kat_prim). */
 int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out);
 
 #ifdef __cplusplus

@@ -232,8 +232,10 @@ def run_reference_dual(prob, state: np.ndarray, tangent: np.ndarray, dts, eta0: 
     return out[0], out[1]
 
 
-def run_kat(func: int, inputs: np.ndarray, nout: int) -> np.ndarray:
-    exe = os.path.join(REF_DIR, "ref_kat")
+def run_kat(func: int, inputs: np.ndarray, nout: int, exe: Optional[str] = None) -> np.ndarray:
+    """Known answers of the reference's point function `func` (``ref_kat``; ``exe``: another
+    build of the same harness, e.g. ``ref_kat_prim`` with mhd_lrstate's primitive reconstruction)."""
+    exe = exe or os.path.join(REF_DIR, "ref_kat")
     inputs = np.ascontiguousarray(inputs, dtype=np.float64)
     ncase, nin = inputs.shape
     with tempfile.TemporaryDirectory(prefix="qaskat_") as td:

@@ -311,30 +311,6 @@ struct LrStencil {
   __device__ __forceinline__ double late(int f, int m) const { return field(f)[c + (m - 2) * s]; }
 };
 
-// mhd_lrstate with the primitive reconstruction mhd_reconst (common/mhd_eigen.c:667-706): each
-// of (ro, vn, vb, vc, cb, cc, pr) interpolated on its own, then the positivity fallback
-// (common/mhd_func.c:150-160)
-template <int ODR, class ST>
-__device__ __forceinline__ void face_states_prim(const ST &st, double vl[7], double vr[7])
-{
-#pragma unroll
-  for (int f = 0; f < 7; f++) {
-    const double w[5] = {st(f, 0), st(f, 1), st(f, 2), st(f, 3), st(f, 4)};
-    nl_lr<ODR>(w, vl[f], vr[f]);
-  }
-  const double eps = 1e-12;
-  if (vl[0] <= eps || vl[6] <= eps) {
-    vl[0] = st(0, 2);
-    vl[1] = st(1, 2);
-    vl[6] = st(6, 2);
-  }
-  if (vr[0] <= eps || vr[6] <= eps) {
-    vr[0] = st(0, 2);
-    vr[1] = st(1, 2);
-    vr[6] = st(6, 2);
-  }
-}
-
 // PR: the face-value form, 0 characteristic, 1 primitive, -1 chosen at run time by v.recon (the
 // forms whose instances may differ per launch); the default kernels take it as a template
 // argument so the characteristic code is compiled without the other branch

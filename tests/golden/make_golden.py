@@ -54,7 +54,7 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
         a = rng.normal(0, 1, (n, 5))
         a[::7] = a[::7, :1]       # constant stencils
         return a
-    if kind == "lrstate":
+    if kind in ("lrstate", "lrstate_prim"):
         ro = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.1
         rest = rng.normal(0, 1, (n, 25))
         pr = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.05
@@ -69,7 +69,7 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
 
 
 KAT_FUNCS = {"flux": ([0, 1, 2, 3], 7), "interp": (list(range(10, 20)), 2), "lrstate": ([20, 21, 22, 23], 14),
-             "cuct": ([30], 1)}
+             "lrstate_prim": ([24, 25, 26, 27], 14), "cuct": ([30], 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -138,12 +138,25 @@ STEP_CASES = [
 ]
 
 
+def make_kat_prim() -> None:
+    """mhd_lrstate with the primitive reconstruction: the harness's ids 20..23 built against
+    mhd_reconst (oracle/_ref/ref_kat_prim), stored as 24..27 (the oracle's ids for that form)."""
+    inp = kat_inputs("lrstate_prim")
+    exe = os.path.join(R.REF_DIR, "ref_kat_prim")
+    outs = {f"f{f + 4}": R.run_kat(f, inp, 14, exe=exe) for f in (20, 21, 22, 23)}
+    np.savez_compressed(os.path.join(OUT, "kat_lrstate_prim.npz"), input_sha=sha(inp), **outs)
+    print("kat lrstate_prim", inp.shape)
+
+
 def main() -> None:
     for name, (funcs, nout) in KAT_FUNCS.items():
+        if name == "lrstate_prim":
+            continue
         inp = kat_inputs(name)
         outs = {f"f{f}": R.run_kat(f, inp, nout) for f in funcs}
         np.savez_compressed(os.path.join(OUT, f"kat_{name}.npz"), input_sha=sha(inp), **outs)
         print("kat", name, inp.shape)
+    make_kat_prim()
     data = {}
     for name, build, mode, nsteps in STEP_CASES:
         p = build()

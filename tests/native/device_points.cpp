@@ -1,6 +1,7 @@
 // Host build of the device point functions of the step (qas_device.cuh is host+device): the
 // Riemann solvers, the face interpolations, the characteristic face states (both the
-// per-field and the grouped-stencil forms the kernels use) and the CUCT weight, with the
+// per-field and the grouped-stencil forms the kernels use), the primitive-variable face states
+// and the CUCT weight, with the
 // argument layout of the known-answer vectors of the reference's own point functions.
 #include "qas_device.cuh"
 
@@ -69,6 +70,18 @@ void t_face_states(int odr, int grouped, const double *a, double *o)
     case 2: face_states_of<2>(a, grouped, o); break;
     case 3: face_states_of<3>(a, grouped, o); break;
     default: face_states_of<4>(a, grouped, o); break;
+  }
+}
+
+// the same with the primitive reconstruction (mhd_reconst): each field interpolated on its own
+void t_face_states_prim(int odr, const double *a, double *o)
+{
+  const ArrayStencil st{a};
+  switch (odr) {
+    case 1: face_states_prim<1>(st, &o[0], &o[7]); break;
+    case 2: face_states_prim<2>(st, &o[0], &o[7]); break;
+    case 3: face_states_prim<3>(st, &o[0], &o[7]); break;
+    default: face_states_prim<4>(st, &o[0], &o[7]); break;
   }
 }
 

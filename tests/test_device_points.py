@@ -6,7 +6,8 @@ square root) is compared with the known-answer vectors of the reference's point 
 (tests/golden/kat_*.npz, from common/mhd_flux.c, common/common_interp.c, common/mhd_func.c
 built from source): the four Riemann solvers, the linear and nonlinear face interpolations the
 schemes use, the characteristic face states of mhd_lrstate at every order -- the per-field
-form and the grouped-stencil form the kernels run -- and the CUCT weight."""
+form and the grouped-stencil form the kernels run --, the primitive-variable face states of
+its mhd_reconst form (qas_scheme.char_mode = 1) and the CUCT weight."""
 import ctypes
 import os
 import shutil
@@ -38,6 +39,7 @@ def dev(tmp_path_factory):
     for f in (lib.t_flux, lib.t_lin, lib.t_nl):
         f.argtypes = [ctypes.c_int, D, D]
     lib.t_face_states.argtypes = [ctypes.c_int, ctypes.c_int, D, D]
+    lib.t_face_states_prim.argtypes = [ctypes.c_int, D, D]
     return lib
 
 
@@ -71,6 +73,15 @@ def test_characteristic_face_states(dev, odr, grouped):
     inp = G.kat_inputs("lrstate")
     gold = np.load(os.path.join(GOLD, "kat_lrstate.npz"))[f"f{19 + odr}"]
     assert_bitwise(_run(dev.t_face_states, inp, 14, odr, grouped), gold, f"mhd_lrstate order {odr} grouped {grouped}")
+
+
+@pytest.mark.parametrize("odr", [1, 2, 3, 4])
+def test_primitive_face_states(dev, odr):
+    """mhd_lrstate with mhd_reconst (the reference's known answers from the harness built against
+    it), the device face_states_prim of qas_scheme.char_mode = 1."""
+    inp = G.kat_inputs("lrstate_prim")
+    gold = np.load(os.path.join(GOLD, "kat_lrstate_prim.npz"))[f"f{23 + odr}"]
+    assert_bitwise(_run(dev.t_face_states_prim, inp, 14, odr), gold, f"primitive face states order {odr}")
 
 
 def test_cuct_weight(dev):
