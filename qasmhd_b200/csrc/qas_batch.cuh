@@ -69,8 +69,11 @@ __global__ void kb_dv(const View *__restrict__ views, BMap map)
 
 // PR: the face-value form of every instance (0 characteristic, 1 primitive) or -1 (mixed: each
 // instance's View decides)
+#ifndef QAS_BATCH_LR_MINB
+#define QAS_BATCH_LR_MINB QAS_LR_MINB
+#endif
 template <int ODR, int A, int PR>
-__global__ void __launch_bounds__(128, QAS_LR_MINB) kb_lr(const View *__restrict__ views, BMap map)
+__global__ void __launch_bounds__(128, QAS_BATCH_LR_MINB) kb_lr(const View *__restrict__ views, BMap map)
 {
   QAS_BATCH_BLOCKS(map)
   if (QAS_BATCH_CELL_OK) {

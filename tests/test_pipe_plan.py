@@ -113,3 +113,12 @@ def test_invalid_arguments():
         L.pipe_plan(2 * GH, 8)
     with pytest.raises(L.QasError):
         L.pipe_plan(264, 65)
+
+
+def test_record_size_matches_the_header():
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    txt = open(os.path.join(root, "include", "qas.h")).read()
+    assert int(re.search(r"#define QAS_PIPE_ITEM_INTS (\d+)", txt)[1]) == L.PIPE_ITEM_INTS == 2 + 2 * 2 * len(
+        L.PIPE_RANGE_NAMES)
