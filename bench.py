@@ -1,13 +1,16 @@
 """Benchmark: qasMHD per-step update in Mcell-updates/s (FP64) on B200.
 
-Default workload (N=1): 2D Orszag-Tang vortex 1024^2, HLLD + characteristic
-WCNS4 + CUCT-weighted CT + SSP-RK3, CFL 0.4, dt refreshed every 2nd step as in
-exec_.  One "step" = one full RK3 time step of the whole grid.  Under torchrun
-(N>1) every rank advances its own independent replica (the plain path is a
-single domain; replicas only), so per-GPU work is fixed: weak scaling.
+Default workload (N=1): 3D low-Mach Kelvin-Helmholtz 256^3 (M = 0.01, beta = 100),
+MLAU flux + characteristic WCNS4 + CUCT-weighted CT + SSP-RK3, CFL 0.4, dt refreshed
+every 2nd step as in exec_ -- the largest single-GPU configuration and the one the
+plain FP64 path is judged on.  One "step" = one full RK3 time step of the whole grid.
+The timed region is K steps; it is timed `--windows` times and the median window is
+the reported value.  Under torchrun (N>1) every rank advances its own independent
+replica (the plain path is a single domain; replicas only), so per-GPU work is
+fixed: weak scaling.
 
---impl reference runs the reference's own OpenMP code, compiled from its
-sources (oracle/_ref), on the host cores for the same workload.
+--impl reference runs the reference's own OpenMP code, compiled from its sources
+(oracle/_ref), on the host's physical cores for the same workload and config.
 
 Prints one JSON line (rank 0).
 """
@@ -28,44 +31,59 @@ import numpy as np  # noqa: E402
 
 ALG_BYTES_PER_CELL_UPDATE = 512  # 8 FP64 fields: stage 1 reads u^n, writes; stages 2-3 read stage input + u^n, write
 
-# Dominant kernel k_lr (characteristic WCNS face states of one direction): algorithmic
-# FP64 arrays per cell: reads ro,vn,vt,vu,bt,bu,pr, the centre normal field and the face
-# normal field (9); writes the 7+7 face states and the CUCT induction states (2 in 2D,
-# 4 in 3D).
-K_LR_ARRAYS = {1: 8 + 14, 2: 9 + 16, 3: 9 + 18}
+# Algorithmic FP64 arrays per cell and launch of the kernels that can dominate a step
+# (reads + writes, each array streamed once):
+#   k_lr     reads ro,vn,vt,vu,bt,bu,pr, the centre normal field and the face normal field (9);
+#            writes the 7+7 face states and the CUCT induction states (2 in 2D, 4 in 3D)
+#   k_flux   reads the 7+7 face states, the face normal field, the induction states (2/4), vn
+#            and the shock detector (MLAU/LHLLD: 1 in 2D, 2 in 3D); writes 8 fluxes and the
+#            central induction fluxes (1 in 2D, 2 in 3D)
+#   k_sweep  (face states + flux of one axis in one kernel) reads the 7 stencil fields, the
+#            centre and face normal fields, the shock detector; writes the fluxes and central
+#            induction fluxes: the face states never leave the SM
+KERNEL_ARRAYS = {
+    "k_lr": {1: 8 + 14, 2: 9 + 16, 3: 9 + 18},
+    "k_flux": {1: 15 + 8, 2: 14 + 1 + 2 + 2 + 8 + 1, 3: 14 + 1 + 4 + 3 + 8 + 2},
+    "k_sweep": {1: 8 + 8, 2: 9 + 1 + 8 + 1, 3: 9 + 2 + 8 + 2},
+}
 # FP64 work of k_lr per cell, counted by ncu on the 2D Orszag-Tang 1024^2 workload
 # (ODR=4; profiles/k_lr_ot2d_1024.md): dadd + dmul + dfma instructions and flops
 # (a dfma counts 2).
 K_LR_FP64_INSTR_PER_CELL = 1054.0
 K_LR_FP64_FLOPS_PER_CELL = 1262.0
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_lr launch (y direction) on the
-# same workload (profiles/k_lr_ot2d_1024.md)
-K_LR_TRAFFIC_PER_LAUNCH = {"ot2d_1024": 76.70e6 + 92.25e6,
-                           # KH 128^3 capture (x faces, 136^3 padded cells: 200.12 + 314.29 MB),
-                           # scaled by padded cells to 264^3 (traffic per cell is size-independent:
-                           # every array is streamed once, the 126 MB L2 holds no full array)
-                           "kh3d_256": (200.12e6 + 314.29e6) * (264 / 136) ** 3}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel, per
+# workload: k_lr (y faces) of OT 1024^2 (profiles/k_lr_ot2d_1024.md) and of KH 3D: the KH 128^3
+# capture (x faces, 136^3 padded cells: 200.12 + 314.29 MB) scaled by padded cells to 264^3
+# (traffic per cell is size-independent: every array is streamed once, the 126 MB L2 holds no
+# full array)
+KERNEL_TRAFFIC_PER_LAUNCH = {("k_lr", "ot2d_1024"): 76.70e6 + 92.25e6,
+                             ("k_lr", "kh3d_256"): (200.12e6 + 314.29e6) * (264 / 136) ** 3}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--windows", type=int, default=5, help="timed windows of --steps steps; the median is reported")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ot2d_1024", "kh3d_256", "kh3d_128", "bw1d_1024"], default="ot2d_1024")
+    ap.add_argument("--workload", choices=["kh3d_256", "ot2d_1024", "kh3d_128", "bw1d_1024"], default="kh3d_256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=None,
+                    help="full RK3 steps of the reference's OpenMP build in cpu_baseline (default: 10 in 3D, 3 else)")
     ap.add_argument("--lr-staging", type=int, choices=[0, 1], default=None,
                     help="reconstruction stencils: 1 = TMA-staged in shared memory, 0 = global loads "
                          "(default: the library's default for the grid)")
+    ap.add_argument("--fused-sweep", type=int, choices=[0, 1], default=None,
+                    help="face states + flux of an axis in one kernel (1) or two (0); default: the library's")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-ensemble", action="store_true")
-    ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-decomposed", action="store_true",
                     help="skip the slab-decomposition leg (KH 256^3 in 4 z-slabs on this GPU vs one domain)")
-    ap.add_argument("--no-plain3d", action="store_true",
-                    help="skip the 3D Kelvin-Helmholtz 256^3 leg (GPU vs the reference's OpenMP build)")
+    ap.add_argument("--no-second", action="store_true",
+                    help="skip the second plain workload (2D Orszag-Tang 1024^2 beside the 3D default)")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint comparison over --steps steps (profiling aid)")
     ap.add_argument("--ensemble-only", action="store_true",
@@ -89,7 +107,8 @@ def lr_forms_case():
     print(json.dumps({"lr_forms_case": "ok"}))
 
 
-def make_problem(name):
+def make_problem(name, world=1):
+    """The workload's problem and its config dict; both arms print the same dict."""
     from qasmhd_b200 import problems as P
     if name == "ot2d_1024":
         p = P.orszag_tang(1024)
@@ -106,6 +125,10 @@ def make_problem(name):
     else:
         p = P.brio_wu(1024)
         cfg = {"workload": "brio_wu_1d_1024", "grid": [1024], "solver": "HLLD", "order": "WCNS4", "rk": 3}
+    # working set of the plain path per step: 77 FP64 arrays of nd cells (state, ut, primitives,
+    # face states, fluxes, EMFs), well above the 126 MB L2 for the 2D and 3D workloads
+    cfg["parallelism"] = f"replicas{world}"
+    cfg["l2"] = "no flush: working set per step ~%.2f GB > 126 MB L2" % (77 * p.nd * 8 / 1e9)
     return p, cfg
 
 
@@ -161,21 +184,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sm)}
 
 
-def cpu_baseline(prob, steps=3, threads=None):
-    """The reference's own OpenMP code (oracle/_ref) on a bounded sample of the workload."""
-    from oracle import refcase as R
-    threads = threads or os.cpu_count()
-    if not R.reference_available(prob.dim, prob.ctw):
-        return None
-    r = R.run_reference(prob, R.MODE_RUN, nsteps=steps, nthreads=threads)
-    st = r["step_times"]
-    per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
-    return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
-            "kind": "reference", "cpu": host_cpu(),
-            "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, "
-                      f"reference -O2 -fopenmp, OMP_NUM_THREADS={threads}"}
-
-
 def host_cpu() -> str:
     try:
         with open("/proc/cpuinfo") as f:
@@ -187,29 +195,74 @@ def host_cpu() -> str:
     return "unknown"
 
 
-def cpu_baseline_o3(prob, steps=3, threads=None):
+def host_cores():
+    """(logical CPUs this process may run on, distinct physical cores among them).  Physical
+    cores are told apart by (package id, core id) from sysfs; without sysfs every logical CPU
+    counts as a core."""
+    try:
+        cpus = sorted(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        cpus = list(range(os.cpu_count() or 1))
+    cores = set()
+    for c in cpus:
+        base = f"/sys/devices/system/cpu/cpu{c}/topology/"
+        try:
+            with open(base + "physical_package_id") as f:
+                pk = f.read().strip()
+            with open(base + "core_id") as f:
+                co = f.read().strip()
+            cores.add((pk, co))
+        except OSError:
+            cores.add(("cpu", str(c)))
+    return len(cpus), len(cores)
+
+
+def _cpu_run(prob, steps, exe=None):
+    """Time `steps` full RK3 steps of the reference's OpenMP build on the host's physical
+    cores (OMP_PROC_BIND=close, OMP_PLACES=cores); returns (median step s, threads, logical)."""
+    from oracle import refcase as R
+    logical, physical = host_cores()
+    r = R.run_reference(prob, R.MODE_RUN, nsteps=steps, nthreads=physical, exe=exe, bind=True)
+    st = r["step_times"]
+    per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
+    return per, physical, logical
+
+
+def cpu_baseline(prob, steps):
+    """The reference's own OpenMP code (oracle/_ref, -O2 -fopenmp) on a bounded sample of the
+    workload: `steps` full RK3 steps, median step time."""
+    from oracle import refcase as R
+    if not R.reference_available(prob.dim, prob.ctw):
+        return None
+    per, threads, logical = _cpu_run(prob, steps)
+    return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
+            "logical_cpus": logical, "kind": "reference", "cpu": host_cpu(),
+            "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, reference -O2 "
+                      f"-fopenmp, OMP_NUM_THREADS={threads} (physical cores) OMP_PROC_BIND=close OMP_PLACES=cores"}
+
+
+def cpu_baseline_o3(prob, steps):
     """The same bounded sample through the reference built with its alternative flags
     (Makefile.inc:3, -O3 -march=native: here the host's x86-64 ISA level).  Timing only: FMA
     contraction changes its last bits."""
     from oracle import refcase as R
-    threads = threads or os.cpu_count()
     exe = R.o3_binary(prob.dim)
     if exe is None:
         return None
-    r = R.run_reference(prob, R.MODE_RUN, nsteps=steps, nthreads=threads, exe=exe)
-    st = r["step_times"]
-    per = float(np.median(st)) if len(st) else r["elapsed"] / max(steps, 1)
+    per, threads, logical = _cpu_run(prob, steps, exe=exe)
     return {"value": prob.interior_cells / per / 1e6, "unit": "Mcell-updates/s", "cores": threads,
-            "kind": "reference", "cpu": host_cpu(),
+            "logical_cpus": logical, "kind": "reference", "cpu": host_cpu(),
             "sample": f"{prob.name}: {steps} full RK3 steps, median step time {per:.3f} s, reference "
-                      f"-O3 -march=x86-64-{R.host_isa_level()} -fopenmp, OMP_NUM_THREADS={threads}"}
+                      f"-O3 -march=x86-64-{R.host_isa_level()} -fopenmp, OMP_NUM_THREADS={threads} "
+                      "OMP_PROC_BIND=close"}
 
 
 def ensemble_compare(steps):
     """Batched ensemble (512 seeded 2D instances, log-uniform sides 64..512, half
-    Orszag-Tang/HLLD, half Kelvin-Helmholtz/MLAU) in one launch sequence per step,
-    against the same instances run one after another through the plain path (each
-    with its own graph-captured exec_ loop).  Device time by CUDA events."""
+    Orszag-Tang/HLLD, half Kelvin-Helmholtz/MLAU) in one launch sequence per step, against
+    the same instances run one after another through the plain path: each with its own
+    graph-captured exec_ loop for the same `steps` steps, and with eager launches over
+    min(steps, 20) steps (per-step rate).  Device time by CUDA events."""
     import torch
 
     from qasmhd_b200 import lib as L
@@ -231,11 +284,13 @@ def ensemble_compare(steps):
     ms_b = s0.elapsed_time(s1)
     launches_b = b.kernel_launches() - l0
     b.close()
+    eager_steps = min(steps, 20)
     ms_p = {True: 0.0, False: 0.0}
     launches_p = 0
     for p in probs:
         with L.Context.from_problem(p) as c:
             for graph in (True, False):
+                n = steps if graph else eager_steps
                 c.upload(p.state)
                 c.run_reset()
                 c.run(max_steps=2, flg=1, stop_rule=0, cfl=0.4, use_graph=graph)
@@ -243,30 +298,30 @@ def ensemble_compare(steps):
                 s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 l0 = c.kernel_launches()
                 s0.record(ext)
-                c.run(max_steps=steps, flg=1, stop_rule=0, cfl=0.4, use_graph=graph)
+                c.run(max_steps=n, flg=1, stop_rule=0, cfl=0.4, use_graph=graph)
                 s1.record(ext)
                 s1.synchronize()
-                ms_p[graph] += s0.elapsed_time(s1)
+                ms_p[graph] += s0.elapsed_time(s1) / n
                 if graph:
                     launches_p += c.kernel_launches() - l0
+    ms_b_step = ms_b / steps
     return {"workload": "ensemble_512_2d_64-512_OT-HLLD_KH-MLAU", "instances": len(probs), "cells": cells,
-            "steps": steps, "batched_mcells": cells * steps / ms_b / 1e3,
-            "per_instance_mcells": cells * steps / ms_p[True] / 1e3, "ratio": ms_p[True] / ms_b,
-            "per_instance_eager_mcells": cells * steps / ms_p[False] / 1e3, "ratio_vs_eager": ms_p[False] / ms_b,
-            "batched_launches": launches_b, "per_instance_launches": launches_p,
-            "basis": "ratio: per-instance runs each with its own graph-captured exec_ loop (the strict "
-                     "baseline); ratio_vs_eager: per-instance plain (eager) kernel launches"}
+            "steps": steps, "batched_mcells": cells / ms_b_step / 1e3,
+            "per_instance_mcells": cells / ms_p[True] / 1e3, "ratio": ms_p[True] / ms_b_step,
+            "per_instance_eager_mcells": cells / ms_p[False] / 1e3, "ratio_vs_eager": ms_p[False] / ms_b_step,
+            "eager_steps": eager_steps, "batched_launches": launches_b, "per_instance_launches": launches_p,
+            "basis": "ratio: per-instance runs each with its own graph-captured exec_ loop over the same steps (the "
+                     "strict baseline); ratio_vs_eager: per-instance plain (eager) kernel launches, per-step rate"}
 
 
-def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
-    """3D low-Mach Kelvin-Helmholtz 256^3 (MLAU, WCNS4, CUCT, RK3): device-timed throughput of
-    the graph-captured exec_ loop next to the reference's own OpenMP build on all host cores
-    (a bounded sample of full steps)."""
+def second_workload(name, steps=20, warmup=3, windows=5, cpu_steps=3):
+    """Another plain workload timed like the headline (graph-captured exec_ loop, median of
+    `windows` windows of `steps` steps) beside the reference's OpenMP build on the host's
+    physical cores, with its host round trip (qas_step_host, and the serial composition)."""
     import torch
 
     from qasmhd_b200 import lib as L
-    from qasmhd_b200 import problems as P
-    prob = P.kelvin_helmholtz(3, 256)
+    prob, cfg = make_problem(name)
     with L.Context.from_problem(prob) as ctx:
         ctx.upload(prob.state)
         ctx.run(max_steps=warmup, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
@@ -274,19 +329,21 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
-        a.record(ext)
-        ctx.run(max_steps=steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
-        b.record(ext)
-        b.synchronize()
-        ms = a.elapsed_time(b) / steps
-        prof = ctx.profile(2, flg=1, cfl=prob.cfl)
-        # the host round trip per step (1.18 GB each way): serial phases vs qas_step_host
+        wins = []
+        for _ in range(windows):
+            a.record(ext)
+            ctx.run(max_steps=steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+            b.record(ext)
+            b.synchronize()
+            wins.append(a.elapsed_time(b) / steps)
+        ms = statistics.median(wins)
+        prof = ctx.profile(min(steps, 10), flg=1, cfl=prob.cfl)
         host = torch.empty((8, prob.nd), dtype=torch.float64, pin_memory=True)
         ctx.download_into(host.numpy())
         hptr = host.numpy()
 
         def e2e_ms(fn, n):
-            for _ in range(2):
+            for _ in range(3):
                 fn()
             torch.cuda.synchronize()
             a.record(ext)
@@ -301,14 +358,14 @@ def plain3d_compare(steps=20, warmup=3, cpu_steps=2):
             ctx.run(max_steps=1, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=False)
             ctx.download_into(hptr)
 
-        ms_serial = e2e_ms(serial_step, 3)
-        ms_host = e2e_ms(lambda: ctx.step_host(hptr, hptr, flg=1, stop_rule=0, cfl=prob.cfl), 3)
+        ms_serial = e2e_ms(serial_step, 5)
+        ms_host = e2e_ms(lambda: ctx.step_host(hptr, hptr, flg=1, stop_rule=0, cfl=prob.cfl), 5)
         del host
     gpu = prob.interior_cells / (ms * 1e-3) / 1e6
-    cpu = cpu_baseline(prob, steps=cpu_steps) if cpu_steps > 0 else None
-    cpu3 = cpu_baseline_o3(prob, steps=cpu_steps) if cpu_steps > 0 else None
-    out = {"workload": "kelvin_helmholtz_3d_256^3_M0.01_mlau_wcns4_ct_rk3", "value": gpu,
-           "unit": "Mcell-updates/s", "ms_per_step": ms, "steps": steps,
+    cpu = cpu_baseline(prob, cpu_steps) if cpu_steps > 0 else None
+    cpu3 = cpu_baseline_o3(prob, cpu_steps) if cpu_steps > 0 else None
+    out = {"workload": cfg["workload"], "config": cfg, "value": gpu, "unit": "Mcell-updates/s",
+           "ms_per_step": ms, "steps": steps, "windows_ms_per_step": wins,
            "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
            "cpu_baseline": cpu, "cpu_baseline_o3": cpu3,
            "e2e": {"value": prob.interior_cells / (ms_host * 1e-3) / 1e6, "unit": "Mcell-updates/s",
@@ -402,16 +459,19 @@ def adjoint_compare(nsteps=400, every=20, eta=0.5e-4):
 
 
 def run_reference_arm(args):
+    """The reference's own OpenMP build (oracle/_ref, -O2 -fopenmp, its default flags) on the
+    host's physical cores, W + K full steps of the same workload; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
-    prob, cfg = make_problem(args.workload)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    prob, cfg = make_problem(args.workload, world)
     if rank != 0:
         return
     from oracle import refcase as R
-    threads = os.cpu_count()
     if not R.reference_available(prob.dim, prob.ctw):
         print(json.dumps({"impl": "reference", "unavailable": "reference oracle binaries (oracle/_ref) not built"}))
         return
-    r = R.run_reference(prob, R.MODE_RUN, nsteps=args.warmup + args.steps, nthreads=threads)
+    logical, threads = host_cores()
+    r = R.run_reference(prob, R.MODE_RUN, nsteps=args.warmup + args.steps, nthreads=threads, bind=True)
     st = r["step_times"][args.warmup:]
     total = float(np.sum(st))
     value = prob.interior_cells * len(st) / total / 1e6
@@ -420,15 +480,18 @@ def run_reference_arm(args):
             "ms_per_step": 1e3 * total / len(st), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial state of the named problem)",
             "config": cfg,
-            "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "kind": "reference",
-                             "sample": f"{prob.name}: {args.warmup}+{len(st)} steps, reference -O2 -fopenmp"},
+            "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": threads, "logical_cpus": logical,
+                             "kind": "reference", "cpu": host_cpu(),
+                             "sample": f"{prob.name}: {args.warmup}+{len(st)} full RK3 steps, reference -O2 -fopenmp, "
+                                       f"OMP_NUM_THREADS={threads} (physical cores) OMP_PROC_BIND=close"},
             "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     exe = R.o3_binary(prob.dim)
-    if exe:  # the same steps through the reference's alternative -O3 -march=native flags
-        r3 = R.run_reference(prob, R.MODE_RUN, nsteps=args.warmup + args.steps, nthreads=threads, exe=exe)
-        st3 = r3["step_times"][args.warmup:]
+    if exe:  # a few steps through the reference's alternative -O3 -march=native flags
+        n3 = min(args.steps, 3)
+        r3 = R.run_reference(prob, R.MODE_RUN, nsteps=1 + n3, nthreads=threads, exe=exe, bind=True)
+        st3 = r3["step_times"][1:]
         line["o3_native"] = {"value": prob.interior_cells * len(st3) / float(np.sum(st3)) / 1e6,
-                             "unit": "Mcell-updates/s", "cores": threads,
+                             "unit": "Mcell-updates/s", "cores": threads, "steps": len(st3),
                              "build": f"-O3 -march=x86-64-{R.host_isa_level()} -fopenmp (timing only)"}
     print(json.dumps(line))
 
@@ -464,11 +527,13 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    prob, cfg = make_problem(args.workload)
+    prob, cfg = make_problem(args.workload, world)
     cells = prob.interior_cells
     ctx = L.Context.from_problem(prob, device=local)
     if args.lr_staging is not None:
         ctx.set_option(L.QAS_OPT_LR_STAGING, args.lr_staging)
+    if args.fused_sweep is not None:
+        ctx.set_option(L.QAS_OPT_FUSED_SWEEP, args.fused_sweep)
     ctx.upload(prob.state)
     ext = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
 
@@ -483,21 +548,25 @@ def main():
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = ctx.kernel_launches()
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    start.record(ext)
-    ctx.run(max_steps=args.steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
-    end.record(ext)
-    end.synchronize()
-    barrier()
+    windows = []
+    launches = 0
+    for _ in range(max(1, args.windows)):
+        barrier()
+        l0 = ctx.kernel_launches()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(ext)
+        ctx.run(max_steps=args.steps, flg=1, stop_rule=0, cfl=prob.cfl, use_graph=True)
+        end.record(ext)
+        end.synchronize()
+        barrier()
+        launches = ctx.kernel_launches() - l0
+        t = torch.tensor([start.elapsed_time(end)], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        windows.append(float(t.item()))
     clk = clocks.stop()
-    launches = ctx.kernel_launches() - l0
-    ms = start.elapsed_time(end)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = statistics.median(windows)
     ms_step = ms_max / args.steps
     value = cells * args.steps * world / (ms_max * 1e-3) / 1e6
 
@@ -552,30 +621,23 @@ def main():
     dom_launches, dom_ms = prof[dom]
     dom_ms_launch = dom_ms / dom_launches
     step_prof_ms = sum(v[1] for v in prof.values())
-    lr_cells = prob.nd  # k_lr covers every cell but two ghost layers per side along its axis
-    lr_bytes = K_LR_ARRAYS[prob.dim] * 8.0 * lr_cells
-    achieved = lr_bytes / (dom_ms_launch * 1e-3) / 1e9 if dom == "k_lr" else None
-    fp64_peak = L.fp64_peak_tflops()
-    lr_tflops = K_LR_FP64_FLOPS_PER_CELL * lr_cells / (dom_ms_launch * 1e-3) / 1e12
-    lr_pipe = K_LR_FP64_INSTR_PER_CELL * lr_cells / (dom_ms_launch * 1e-3) / (fp64_peak * 1e12 / 2.0)
+    dom_cells = prob.nd  # the face kernels cover every cell but two ghost layers per side along their axis
+    arrays = KERNEL_ARRAYS.get(dom, {}).get(prob.dim)
+    achieved = arrays * 8.0 * dom_cells / (dom_ms_launch * 1e-3) / 1e9 if arrays else None
     line = {
         "metric": "Mcell-updates/s/GPU FP64 (per-step update)", "value": value, "unit": "Mcell-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "windows": len(windows), "windows_ms": windows, "timing": "median of the timed windows of K steps",
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded initial state of the named problem)",
-        "config": dict(cfg, parallelism=f"replicas{world}",
-                       l2="working set per step ~%.2f GB > 126 MB L2" % (77 * prob.nd * 8 / 1e9)),
+        "config": cfg,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": (achieved / hbm_peak) if achieved else None,
-                     "traffic": K_LR_TRAFFIC_PER_LAUNCH.get(args.workload),
+                     "traffic": KERNEL_TRAFFIC_PER_LAUNCH.get((dom, args.workload)),
                      "launch_ms": dom_ms_launch, "share_of_step": dom_ms / step_prof_ms,
-                     "basis": f"algorithmic {K_LR_ARRAYS[prob.dim]} FP64 arrays per cell per launch / live "
+                     "basis": f"algorithmic {arrays} FP64 arrays per cell per launch x {dom_cells} cells / live "
                               f"CUDA-event launch time; peak of {peak_src}; traffic = ncu dram read+write "
                               "per launch"},
-        "fp64": {"kernel": "k_lr", "achieved_tflops": lr_tflops, "peak_tflops": fp64_peak,
-                 "frac": lr_tflops / fp64_peak, "pipe_frac": lr_pipe,
-                 "basis": "ncu-counted FP64 flops per cell x cells / live launch time; peak = measured DFMA "
-                          "throughput (qas_fp64_peak); pipe_frac = FP64 instructions vs the DFMA issue rate"},
         "step_roofline": {"achieved": step_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": step_gbs / hbm_peak,
                           "basis": "whole step, 512 algorithmic B per cell-update"},
         "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items()},
@@ -584,24 +646,36 @@ def main():
         "e2e_serial": {"value": e_serial, "unit": "Mcell-updates/s",
                        "api": "qas_upload_block + qas_run(1 step) + qas_download_block"},
         "gpu_launches": launches,
+        "gpu_launches_basis": "kernel launches of one timed window of K steps",
         "clocks": clk,
     }
+    if "k_lr" in prof:
+        fp64_peak = L.fp64_peak_tflops()
+        lr_launches, lr_ms = prof["k_lr"]
+        lr_ms_launch = lr_ms / lr_launches
+        lr_tflops = K_LR_FP64_FLOPS_PER_CELL * prob.nd / (lr_ms_launch * 1e-3) / 1e12
+        lr_pipe = K_LR_FP64_INSTR_PER_CELL * prob.nd / (lr_ms_launch * 1e-3) / (fp64_peak * 1e12 / 2.0)
+        line["fp64"] = {"kernel": "k_lr", "achieved_tflops": lr_tflops, "peak_tflops": fp64_peak,
+                        "frac": lr_tflops / fp64_peak, "pipe_frac": lr_pipe,
+                        "basis": "ncu-counted FP64 flops per cell x cells / live launch time; peak = measured DFMA "
+                                 "throughput (qas_fp64_peak); pipe_frac = FP64 instructions vs the DFMA issue rate"}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(prob)
-        line["cpu_baseline_o3"] = cpu_baseline_o3(prob)
+        steps_cpu = args.cpu_steps if args.cpu_steps is not None else (10 if prob.dim == 3 else 3)
+        line["cpu_baseline"] = cpu_baseline(prob, steps_cpu)
+        line["cpu_baseline_o3"] = cpu_baseline_o3(prob, max(2, steps_cpu // 2))
+        if line["cpu_baseline"]:
+            line["ratio_vs_cpu"] = value / line["cpu_baseline"]["value"]
+            line["e2e"]["ratio_vs_cpu"] = e_value / line["cpu_baseline"]["value"]
+    ctx.close()
+    if rank == 0 and not args.no_second and world == 1:
+        other = "ot2d_1024" if args.workload != "ot2d_1024" else "kh3d_256"
+        line["second"] = second_workload(other, cpu_steps=0 if args.no_cpu_baseline else 3)
     if rank == 0 and not args.no_ensemble and world == 1:
-        ctx.close()
         line["batched"] = ensemble_compare(args.ensemble_steps)
     if rank == 0 and not args.no_adjoint and world == 1:
-        ctx.close()
         line["adjoint"] = adjoint_compare()
     if rank == 0 and not args.no_decomposed and world == 1:
-        ctx.close()
         line["decomposed"] = decomposed_compare()
-    if rank == 0 and not args.no_plain3d and world == 1 and args.workload != "kh3d_256":
-        ctx.close()
-        line["plain3d"] = plain3d_compare(cpu_steps=0 if args.no_cpu_baseline else 2)
-    ctx.close()
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:

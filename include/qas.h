@@ -391,12 +391,18 @@ qas_status qas_adjoint_backward(qas_ctx *ctx, const double *dldu_final, double *
  * Allocation-free max |div B| (no counterpart in the reference, whose caller owns host
  * arrays and never allocates device memory): the same value as qas_max_divb, for a state
  * the caller already holds in device memory, without a context and without allocating.
+ * It serves callers whose device memory is all handed to an arena or caching allocator
+ * under a fixed budget (a framework's memory pool), where a library cudaMalloc would fail
+ * or eat into that budget.  It is a synchronous host query: it ends with a device-to-host
+ * copy of the result and synchronises `stream`, so it must not be called while that
+ * stream is being captured into a CUDA graph.
  * d_state: 8 fields of the reference's ghost-padded layout, field m at d_state +
- * m*field_stride (field_stride >= nd); stream: a cudaStream_t (NULL = default stream);
- * synchronises that stream.  Scratch is a static device array sized for
- * QAS_NOALLOC_MAX_ROWS interior rows (nym*nzm); larger grids return QAS_ERR_UNSUPPORTED
- * with the reason in qas_last_cuda_error().  The first call on a device resolves the
- * scratch address (module loading may allocate): make it before any stream capture.
+ * m*field_stride (field_stride >= nd); stream: a cudaStream_t (NULL = default stream).
+ * Scratch is a static 512 KiB device array (every device that loads the library holds it
+ * until exit) sized for QAS_NOALLOC_MAX_ROWS interior rows (nym*nzm); larger grids return
+ * QAS_ERR_UNSUPPORTED with the reason in qas_last_cuda_error().  The first call on a device
+ * loads the module (which may allocate): make it before the allocation-free section.  An
+ * error already pending on the calling thread is returned (QAS_ERR_CUDA) and left pending.
  * Calls that overlap in time on one device share the scratch and race: serialise them.
  * ------------------------------------------------------------------------------------ */
 #define QAS_NOALLOC_MAX_ROWS 65536

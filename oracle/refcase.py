@@ -145,9 +145,11 @@ def read_result(path: str, prob):
 
 
 def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, nthreads: int = 0,
-                  state: Optional[np.ndarray] = None, timeout: float = 3600.0, exe: Optional[str] = None):
+                  state: Optional[np.ndarray] = None, timeout: float = 3600.0, exe: Optional[str] = None,
+                  bind: bool = False):
     """Run the reference's own code on ``prob`` and return its result dict (``exe``: another
-    build of the same driver, e.g. o3_binary(), for timing)."""
+    build of the same driver, e.g. o3_binary(), for timing; ``bind``: pin the OpenMP threads
+    to consecutive cores, OMP_PROC_BIND=close OMP_PLACES=cores)."""
     if getattr(prob, "char_mode", 0):
         variant = "prim"
     elif getattr(prob, "hall", False):
@@ -164,6 +166,9 @@ def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, 
         env = dict(os.environ)
         if nthreads > 0:
             env["OMP_NUM_THREADS"] = str(nthreads)
+        if bind:
+            env["OMP_PROC_BIND"] = "close"
+            env["OMP_PLACES"] = "cores"
         subprocess.run([exe, cin, cout], check=True, env=env, timeout=timeout,
                        stdout=subprocess.DEVNULL)
         return read_result(cout, prob)

@@ -1,8 +1,10 @@
 """qas_max_divb_noalloc: max |div B| of a caller-owned device state with no device
-allocation inside the call, against the context entry point qas_max_divb on the same
-state (same per-cell expression, so the maxima agree to the test tolerance -- in fact
-exactly).  Kept in its own file, named to be collected last, so it also runs after
-every other GPU test in the same process."""
+allocation inside the call, for callers whose device memory belongs to an arena or
+caching allocator under a fixed budget.  Checked against the context entry point
+qas_max_divb on the same state (same per-cell expression, so the maxima agree to the
+test tolerance -- in fact exactly), on two calls in a row, and the device's free memory
+is the same before and after a call.  Kept in its own file, named to be collected last,
+so it also runs after every other GPU test in the same process."""
 import numpy as np
 import pytest
 import torch
@@ -42,7 +44,12 @@ def test_matches_context_entry_point_twice(name, prob, nsteps):
     stream = torch.cuda.current_stream().cuda_stream
     g = _grid(prob)
     first = L.max_divb_noalloc(g, prob.odr, d.data_ptr(), nd, stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
     second = L.max_divb_noalloc(g, prob.odr, d.data_ptr(), nd, stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)  # the second call allocated no device memory
     assert ref > 0.0
     assert abs(first - ref) <= RTOL * ref, (first, ref)
     assert abs(second - ref) <= RTOL * ref, (second, ref)
