@@ -264,6 +264,13 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
 #define QAS_OPT_PIPE_ITEMS 3 /* windows of planes of qas_step_host's wave, 1..64 (default 32) */
 #define QAS_OPT_PIPE_LANES 4 /* streams of qas_step_host's stages, 1..3 (default 3 when their work arrays
                                 fit); set before the first qas_step_host of the context */
+/* Failure-path hook for tests of the bounded waits: value >= 0 makes every CTA of the TMA-staged
+ * reconstruction (QAS_OPT_LR_STAGING = 1) skip the load of its plane number `value`, with each
+ * mbarrier wait bounded at 100 us instead of 2 s, so the wait for that plane runs out: the kernel
+ * latches the error, waits for its own loads in flight, returns, and the next synchronising call
+ * reports QAS_ERR_TIMEOUT (the state is then not a valid step).  value < 0 restores the defaults.
+ * QAS_ERR_UNSUPPORTED where the staged form is not available. */
+#define QAS_OPT_TEST_TMA_STALL 5
 qas_status qas_set_option(qas_ctx *ctx, int option, int value);
 
 /* Thread-block tile (tx*ty*tz <= 128 threads, tx a multiple of 32) of one cell kernel

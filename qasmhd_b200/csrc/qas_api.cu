@@ -92,6 +92,7 @@ struct qas_ctx {
   // face sweep form: two kernels with the face states in HBM (default, measured faster on
   // B200: both halves are latency/FP64-bound, the fused kernel spills) or one fused kernel
   bool fused = false;
+  int sweep_seg[3] = {0, 0, 0};  // segment length of the fused y / z sweeps (0: not chosen yet)
   // live per-kernel timing (qas_profile_run): an event pair around every launch
   bool prof = false;
   std::vector<cudaEvent_t> prof_events;
@@ -259,11 +260,11 @@ namespace {
 
 enum Kid {
   KID_PRIM, KID_DV, KID_LR, KID_FLUX, KID_EMF, KID_UPDATE, KID_BOUND, KID_BEGIN, KID_VMAX, KID_SETDT,
-  KID_DVEL, KID_ERES, KID_DFLUX, KID_DUPDATE, KID_DBOUND, KID_DCOPY, KID_DSUB, KID_COUNT
+  KID_DVEL, KID_ERES, KID_DFLUX, KID_DUPDATE, KID_DBOUND, KID_DCOPY, KID_DSUB, KID_SWEEP, KID_COUNT
 };
 const char *const KID_NAMES[KID_COUNT] = {"k_prim", "k_dv", "k_lr", "k_flux", "k_emf", "k_update", "k_bound",
                                           "k_begin_step", "k_vmax", "k_setdt", "k_dvel", "k_eres", "k_dflux",
-                                          "k_dupdate", "k_dbound", "k_dcopy", "k_dsub"};
+                                          "k_dupdate", "k_dbound", "k_dcopy", "k_dsub", "k_sweep"};
 
 void prof_mark(qas_ctx *c, int kid)
 {
@@ -411,6 +412,8 @@ bool setup_lr_tma(qas_ctx *c)
       }
     }
     p.seg = bseg;
+    p.wait_ns = 2000000000ull;  // 2 s of device time per mbarrier wait
+    p.stall_plane = -1;
     p.ms = (len + bseg - 1) / bseg;
     p.items = p.xt * p.rt * p.ms;
     c->lr_grid[a] = (int)std::min<long long>(p.items, slots);
@@ -470,19 +473,83 @@ void launch_flux(qas_ctx *c, int a)
   }
 }
 
+// segment length of the y / z sweeps: fewest cell computations per resident block slot over
+// the waves of blocks (each segment recomputes the cell before its first face)
+int sweep_seg(qas_ctx *c, int a, const void *fn)
+{
+  if (c->sweep_seg[a] > 0) return c->sweep_seg[a];
+  const Geo &g = c->geo;
+  int dev = 0, sms = 148, occ = 1;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  const long long colb = ((long long)g.nx * (a == 1 ? g.nz : g.ny) + 127) / 128;
+  const long long slots = (long long)sms * occ;
+  const int len = g.n[a] - 5;  // faces 3 .. n-3
+  double best = 1e300;
+  int bseg = len;
+  for (int ns = 1; ns <= len; ns++) {
+    const int seg = (len + ns - 1) / ns;
+    const long long blocks = colb * ((len + seg - 1) / seg);
+    const double cost = (double)((blocks + slots - 1) / slots) * (seg + 1);
+    if (cost < best - 1e-9) {
+      best = cost;
+      bseg = seg;
+    }
+  }
+  c->sweep_seg[a] = bseg;
+  return bseg;
+}
+
+// choose the y / z segment lengths outside any stream capture (occupancy query)
+template <int ODR, int RMN>
+void sweep_prepare_t(qas_ctx *c)
+{
+  if (c->geo.dim >= 2) sweep_seg(c, 1, (const void *)k_sweep_m<ODR, RMN, 1>);
+  if (c->geo.dim >= 3) sweep_seg(c, 2, (const void *)k_sweep_m<ODR, RMN, 2>);
+}
+template <int ODR>
+void sweep_prepare_o(qas_ctx *c)
+{
+  switch (c->scheme.rmn) {
+    case 0: sweep_prepare_t<ODR, 0>(c); break;
+    case 1: sweep_prepare_t<ODR, 1>(c); break;
+    case 2: sweep_prepare_t<ODR, 2>(c); break;
+    default: sweep_prepare_t<ODR, 3>(c); break;
+  }
+}
+void sweep_prepare(qas_ctx *c)
+{
+  switch (c->scheme.odr) {
+    case 1: sweep_prepare_o<1>(c); break;
+    case 2: sweep_prepare_o<2>(c); break;
+    case 3: sweep_prepare_o<3>(c); break;
+    default: sweep_prepare_o<4>(c); break;
+  }
+}
+
 template <int ODR, int RMN>
 void launch_sweep(qas_ctx *c, int a)
 {
   const Geo &g = c->geo;
   if (a == 0) {
-    const unsigned nb = (unsigned)((g.nx - 5 + 4 * 31 - 1) / (4 * 31));
-    QL(c, KID_LR, k_sweep_x<ODR, RMN><<<dim3(nb, g.ny, g.nz), 128, 0, c->stream>>>(c->view));
-  } else if (a == 1) {
-    const unsigned ns = (unsigned)((g.ny - 5 + QAS_SWEEP_SEG - 1) / QAS_SWEEP_SEG);
-    QL(c, KID_LR, k_sweep_m<ODR, RMN, 1><<<dim3((g.nx + 127) / 128, ns, g.nz), 128, 0, c->stream>>>(c->view));
+    // warp w takes flattened cells [31w, 31w+32); the last cell needing a flux is total-1
+    const long long total = (long long)(g.nx - 4) * g.ny * g.nz;
+    const long long nwarps = (total - 2) / 31 + 1;
+    const unsigned nb = (unsigned)((nwarps + 3) / 4);
+    QL(c, KID_SWEEP, k_sweep_x<ODR, RMN><<<nb, 128, 0, c->stream>>>(c->view, nwarps));
+    return;
+  }
+  const unsigned colb = (unsigned)(((long long)g.nx * (a == 1 ? g.nz : g.ny) + 127) / 128);
+  const int len = g.n[a] - 5;
+  if (a == 1) {
+    const int seg = sweep_seg(c, 1, (const void *)k_sweep_m<ODR, RMN, 1>);
+    QL(c, KID_SWEEP, k_sweep_m<ODR, RMN, 1><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
   } else {
-    const unsigned ns = (unsigned)((g.nz - 5 + QAS_SWEEP_SEG - 1) / QAS_SWEEP_SEG);
-    QL(c, KID_LR, k_sweep_m<ODR, RMN, 2><<<dim3((g.nx + 127) / 128, g.ny, ns), 128, 0, c->stream>>>(c->view));
+    const int seg = sweep_seg(c, 2, (const void *)k_sweep_m<ODR, RMN, 2>);
+    QL(c, KID_SWEEP, k_sweep_m<ODR, RMN, 2><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
   }
 }
 
@@ -1450,6 +1517,7 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
       c->graph = nullptr;
     }
     c->fused = f;
+    if (f) sweep_prepare(c);
     return QAS_OK;
   }
   if (option == QAS_OPT_LR_STAGING) {
@@ -1461,6 +1529,19 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
       c->graph = nullptr;
     }
     c->lr_tma = t;
+    return QAS_OK;
+  }
+  if (option == QAS_OPT_TEST_TMA_STALL) {
+    if (!c->lr_tma_ok) return QAS_ERR_UNSUPPORTED;
+    if (c->graph) {  // the captured graph holds the plans by value
+      cudaStreamSynchronize(c->stream);
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+    for (int a = 0; a < 3; a++) {
+      c->lr_plan[a].stall_plane = value >= 0 ? value : -1;
+      c->lr_plan[a].wait_ns = value >= 0 ? 100000ull : 2000000000ull;
+    }
     return QAS_OK;
   }
   if (option == QAS_OPT_PIPE_ITEMS) return pipe_set_items(c, value);

@@ -538,9 +538,15 @@ QAS_HD void flux_hlld(const double L[7], const double R[7], double bnc, double g
   F[6] = (enu + ptc) * vnc - bnc * (vtu * btu + vuu * buu);
 }
 
-// MLAU all-speed flux, common/mhd_flux.c:7-192
-QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double gamma,
-                                          double dv0, double dv1, double F[7])
+// MLAU all-speed flux, common/mhd_flux.c:7-192.  Every value keeps the reference's expression
+// and operation order; only the order of independent statements differs, so that few values are
+// live at once (the kernels run this solver at 80 registers): the first two energy-flux terms are
+// summed as soon as their factors exist, the two transverse components are finished one after
+// the other, and each flux goes to out(m, value) as soon as it is final (the kernels store it at
+// once).  out receives F = (fro, fmn, fmt, fmu, fbt, fbu, fen) in the order 0, 1, 2, 4, 3, 5, 6.
+template <class Out>
+QAS_HD void flux_mlau_out(const double L[7], const double R[7], double bnc, double gamma, double dv0, double dv1,
+                          Out &&out)
 {
   const double rol = L[0], vnl = L[1], vtl = L[2], vul = L[3], btl = L[4], bul = L[5], prl = L[6];
   const double ror = R[0], vnr = R[1], vtr = R[2], vur = R[3], btr = R[4], bur = R[5], prr = R[6];
@@ -573,6 +579,7 @@ QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double g
   double ccl2 = 0.5 * (cbl2 + sqrt(fabs(cbl2 * cbl2 - 4.0 * vl2 * cal2)));
   double ccr2 = 0.5 * (cbr2 + sqrt(fabs(cbr2 * cbr2 - 4.0 * vr2 * car2)));
   double cmax = sqrt(qmax(cfl2, cfr2));
+  double cfmod = sqrt(qmax(ccl2, ccr2));
   double cfn = cmax;
   double cfni = 1.0 / cfn;
   double sl = qmin(0.0, qmin(vnl, vnr) - cmax);
@@ -611,12 +618,14 @@ QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double g
   double dirl = 0.5 * (1.0 + dir);
   double dirr = 1.0 - dirl;
   mflux *= (dirl * rol + dirr * ror);
+  out(0, mflux);
   double mfl = mflux * dirl;
   double mfr = mflux - mfl;
   double ptot = bfl * ptl + bfr * ptr;
-  double cfmod = sqrt(qmax(ccl2, ccr2));
   ptot -= 0.25 * bfl * bfr * (rol + ror) * cfmod * (vnr - vnl);
   ptot -= 0.5 * (1.0 - cfmod * cfni) * (bfl + bfr - 1.0) * (ptl + ptr);
+  out(1, mfl * vnl + mfr * vnr + ptot - 0.5 * bnc2);
+  const double e6 = mfl * hnl + mfr * hnr;  // fen = e6 - bnvb
   double slvl = sl - vnl;
   double srvr = sr - vnr;
   double snc = dirl * sl + dirr * sr;
@@ -628,36 +637,16 @@ QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double g
   double srvci = 1.0 / srvc;
   double rhdl = rol * slvl * slvc - bnc2;
   double rhdr = ror * srvr * srvc - bnc2;
-  double dvtl = 0.0, dvul = 0.0, dbtl = 0.0, dbul = 0.0;
-  double dvtr = 0.0, dvur = 0.0, dbtr = 0.0, dbur = 0.0;
-  if (fabs(rhdl) > QAS_FL_EPS) {
-    double q = (vnc - vnl) / rhdl;
-    dvtl = -bnc * btl * q;
-    dvul = -bnc * bul * q;
-    dbtl = bnc2 * btl * q * slvci;
-    dbul = bnc2 * bul * q * slvci;
-  }
-  if (fabs(rhdr) > QAS_FL_EPS) {
-    double q = (vnc - vnr) / rhdr;
-    dvtr = -bnc * btr * q;
-    dvur = -bnc * bur * q;
-    dbtr = bnc2 * btr * q * srvci;
-    dbur = bnc2 * bur * q * srvci;
-  }
+  // the reference's q of each side, used only where |rhd| > FL_EPS (else the corrections are 0.0)
+  const bool hl = fabs(rhdl) > QAS_FL_EPS, hr = fabs(rhdr) > QAS_FL_EPS;
+  const double ql = hl ? (vnc - vnl) / rhdl : 0.0;
+  const double qr = hr ? (vnc - vnr) / rhdr : 0.0;
   double cmpl = slvl * slvci;
   double cmpr = srvr * srvci;
   double ro2l = rol * cmpl;
   double srol = sqrt(ro2l);
-  double vt2l = dvtl + vtl;
-  double vu2l = dvul + vul;
-  double bt2l = dbtl + btl * cmpl;
-  double bu2l = dbul + bul * cmpl;
   double ro2r = ror * cmpr;
   double sror = sqrt(ro2r);
-  double vt2r = dvtr + vtr;
-  double vu2r = dvur + vur;
-  double bt2r = dbtr + btr * cmpr;
-  double bu2r = dbur + bur * cmpr;
   double sroi = 1.0 / (srol + sror);
   double srollri = srol * sroi;
   double srorlri = sror * sroi;
@@ -668,35 +657,47 @@ QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double g
   double bnsrv = qmax(bnca - dir * vnc * (dirl * srol + dirr * sror), 0.0);
   double ccb = sroi * bnsrv;
   double ccv = srol * sror * ccb;
-  double bnvt = bnflb * vt2l + bnfrb * vt2r + ccb * (bt2r - bt2l);
-  double bnvu = bnflb * vu2l + bnfrb * vu2r + ccb * (bu2r - bu2l);
-  double bnbt = bnflv * bt2l + bnfrv * bt2r + ccv * (vt2r - vt2l);
-  double bnbu = bnflv * bu2l + bnfrv * bu2r + ccv * (vu2r - vu2l);
-  bnvt -= vnc * (dirl * dbtl + dirr * dbtr);
-  bnvu -= vnc * (dirl * dbul + dirr * dbur);
-  bnbt -= mflux * (dirl * dvtl + dirr * dvtr);
-  bnbu -= mflux * (dirl * dvul + dirr * dvur);
-  double fmt = mfl * vtl + mfr * vtr - bnbt;
-  double fmu = mfl * vul + mfr * vur - bnbu;
-  double fbt = mfl * btl * roli + mfr * btr * rori - bnvt;
-  double fbu = mfl * bul * roli + mfr * bur * rori - bnvu;
-  F[0] = mflux;
-  F[1] = mfl * vnl + mfr * vnr + ptot - 0.5 * bnc2;
-  F[2] = fmt;
-  F[3] = fmu;
-  F[4] = fbt;
-  F[5] = fbu;
   double vb1 = dirl * (vtl * btl + vul * bul) + dirr * (vtr * btr + vur * bur);
-  double vb2 = dirl * (vt2l * bt2l + vu2l * bu2l) + dirr * (vt2r * bt2r + vu2r * bu2r);
+  // one transverse component (t: vt, bt; u: vu, bu): its momentum and induction fluxes, its
+  // terms of vb2 (v2*b2 of each side) and its term of vb3's numerator
+  auto comp = [&](double vl_, double bl_, double vr_, double br_, int mf, int mb, double &pl, double &pr,
+                  double &q3) {
+    const double dvl = hl ? -bnc * bl_ * ql : 0.0;
+    const double dbl = hl ? bnc2 * bl_ * ql * slvci : 0.0;
+    const double dvr = hr ? -bnc * br_ * qr : 0.0;
+    const double dbr = hr ? bnc2 * br_ * qr * srvci : 0.0;
+    const double v2l = dvl + vl_;
+    const double b2l = dbl + bl_ * cmpl;
+    const double v2r = dvr + vr_;
+    const double b2r = dbr + br_ * cmpr;
+    double bnv = bnflb * v2l + bnfrb * v2r + ccb * (b2r - b2l);
+    double bnb = bnflv * b2l + bnfrv * b2r + ccv * (v2r - v2l);
+    bnv -= vnc * (dirl * dbl + dirr * dbr);
+    bnb -= mflux * (dirl * dvl + dirr * dvr);
+    const double fm = mfl * vl_ + mfr * vr_ - bnb;
+    const double fb = mfl * bl_ * roli + mfr * br_ * rori - bnv;
+    out(mf, fm);
+    out(mb, fb);
+    pl = v2l * b2l;
+    pr = v2r * b2r;
+    q3 = (fm * vnc + fb * bnc) * (fm * bnc + fb * mflux);
+  };
+  double plt, prt, q3t, plu, pru, q3u;
+  comp(vtl, btl, vtr, btr, 2, 4, plt, prt, q3t);
+  comp(vul, bul, vur, bur, 3, 5, plu, pru, q3u);
+  double vb2 = dirl * (plt + plu) + dirr * (prt + pru);
   double rv2b2 = (mflux * vnc - bnc2);
   rv2b2 *= rv2b2;
   double vb3 = 0.0;
-  if (rv2b2 > QAS_FL_EPS * QAS_FL_EPS) {
-    vb3 = (+(fmt * vnc + fbt * bnc) * (fmt * bnc + fbt * mflux) + (fmu * vnc + fbu * bnc) * (fmu * bnc + fbu * mflux)) /
-          rv2b2;
-  }
+  if (rv2b2 > QAS_FL_EPS * QAS_FL_EPS) vb3 = (q3t + q3u) / rv2b2;
   double bnvb = sgn * (bnca * (snc * vb2 - vnc * vb1) * (dirl * slvci + dirr * srvci) + bnsrv * (vb3 - vb2));
-  F[6] = mfl * hnl + mfr * hnr - bnvb;
+  out(6, e6 - bnvb);
+}
+
+QAS_HD void flux_mlau(const double L[7], const double R[7], double bnc, double gamma, double dv0, double dv1,
+                      double F[7])
+{
+  flux_mlau_out(L, R, bnc, gamma, dv0, dv1, [&](int m, double x) { F[m] = x; });
 }
 
 // Roe flux, common/mhd_flux.c:194-433
@@ -874,6 +875,22 @@ QAS_HD void riemann(const double L[7], const double R[7], double bnc, double gam
     flux_hlld<true>(L, R, bnc, gamma, dv0, dv1, F);
   else
     flux_mlau(L, R, bnc, gamma, dv0, dv1, F);
+}
+
+// the same flux handed to out(m, F[m]) as each component is final (MLAU emits while it runs;
+// the other solvers after their last component)
+template <int RMN, class Out>
+QAS_HD void riemann_out(const double L[7], const double R[7], double bnc, double gamma, double dv0, double dv1,
+                        Out &&out)
+{
+  if constexpr (RMN == 3) {
+    flux_mlau_out(L, R, bnc, gamma, dv0, dv1, out);
+  } else {
+    double F[7];
+    riemann<RMN>(L, R, bnc, gamma, dv0, dv1, F);
+#pragma unroll
+    for (int m = 0; m < 7; m++) out(m, F[m]);
+  }
 }
 
 // CUCT corner weight, common/mhd_func.c:56-76. Arguments are the values at the

@@ -376,6 +376,46 @@ __global__ void __launch_bounds__(128, QAS_LR_MINB) k_lr(View v)
 // ---------------------------------------------------------------------------
 // Riemann flux per face along axis A (mhd2d_solve.cpp:172-199 and 3D analogues)
 // ---------------------------------------------------------------------------
+// Stores one face's fluxes as the solver finishes them: F[0..3] to the mass and momentum fluxes
+// (normal component at 1+A), F[4] / F[5] minus the central part of the induction flux (also
+// stored, fc), F[6] plus the work of gravity.  The central parts come from the induction states
+// of the two cells: loaded here (LOADQ, the split form) or handed over in registers (fused).
+template <int A, bool LOADQ>
+struct FaceSink {
+  const View &v;
+  long long f, s;
+  double ql0, qr0, ql1, qr1;  // induction states when !LOADQ
+  double f0;
+  __device__ __forceinline__ double central(int t)
+  {
+    const double l = LOADQ ? v.ql[t][f - s] : (t == 0 ? ql0 : ql1);
+    const double r = LOADQ ? v.qr[t][f] : (t == 0 ? qr0 : qr1);
+    const double fc = 0.5 * (l + r);
+    v.fc[A][t][f] = fc;
+    return fc;
+  }
+  __device__ __forceinline__ void operator()(int m, double x)
+  {
+    constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
+    const int dim = v.g.dim;
+    switch (m) {
+      case 0:
+        v.f[A][0][f] = x;
+        f0 = x;
+        break;
+      case 1: v.f[A][1 + A][f] = x; break;
+      case 2: v.f[A][1 + B][f] = x; break;
+      case 3: v.f[A][1 + C][f] = x; break;
+      case 4: v.f[A][4 + B][f] = (dim == 3 || (dim == 2 && A == 0)) ? x - central(0) : x; break;
+      case 5: v.f[A][4 + C][f] = (dim == 3 || (dim == 2 && A == 1)) ? x - central(1) : x; break;
+      default:
+        // work done by gravity (2D/SERIAL/RTI/mhd2d_solve.cpp:197, :305; 3D/MPI/RTI/mhd3d_solve.cpp:247, :412, :577)
+        v.f[A][7][f] = v.phi ? x + f0 * 0.5 * (v.phi[f - s] + v.phi[f]) : x;
+        break;
+    }
+  }
+};
+
 template <int RMN, int A>
 __device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
 {
@@ -386,7 +426,7 @@ __device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
   const long long f = cidx(g, i, j, k);
   const long long s = g.s[A];
   constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
-  double L[7], R[7], F[7];
+  double L[7], R[7];
 #pragma unroll
   for (int m = 0; m < 7; m++) {
     L[m] = v.vl[m][f - s];
@@ -406,28 +446,7 @@ __device__ __forceinline__ void flux_body(const View &v, int i, int j, int k)
       dv1 = qmin(qmin(d1[f - s], d1[f]), qmin(d2[f - s], d2[f]));
     }
   }
-  riemann<RMN>(L, R, bn, v.gam, dv0, dv1, F);
-  v.f[A][0][f] = F[0];
-  v.f[A][1 + A][f] = F[1];
-  v.f[A][1 + B][f] = F[2];
-  v.f[A][1 + C][f] = F[3];
-  double fbt = F[4], fbu = F[5];
-  if (g.dim >= 2) {
-    if (g.dim == 3 || A == 0) {
-      const double fc0 = 0.5 * (v.ql[0][f - s] + v.qr[0][f]);
-      v.fc[A][0][f] = fc0;
-      fbt -= fc0;
-    }
-    if (g.dim == 3 || A == 1) {
-      const double fc1 = 0.5 * (v.ql[1][f - s] + v.qr[1][f]);
-      v.fc[A][1][f] = fc1;
-      fbu -= fc1;
-    }
-  }
-  v.f[A][4 + B][f] = fbt;
-  v.f[A][4 + C][f] = fbu;
-  // work done by gravity (2D/SERIAL/RTI/mhd2d_solve.cpp:197, :305; 3D/MPI/RTI/mhd3d_solve.cpp:247, :412, :577)
-  v.f[A][7][f] = v.phi ? F[6] + F[0] * 0.5 * (v.phi[f - s] + v.phi[f]) : F[6];
+  riemann_out<RMN>(L, R, bn, v.gam, dv0, dv1, FaceSink<A, true>{v, f, s, 0.0, 0.0, 0.0, 0.0, 0.0});
 }
 // resident-block caps of the flux kernel per solver, measured on B200 per launch: Roe at 4
 // (128 registers, from 162) 0.0906 -> 0.0782 ms (KH 2D 1024^2); HLLD at 8 (64 registers, a
@@ -466,17 +485,25 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) k_flux_mlau(View v)
 // ---------------------------------------------------------------------------
 // Fused face sweep along axis A: characteristic face states of every cell and
 // the Riemann flux of every face in one kernel, so the face states never go
-// through HBM.  Along x a warp covers 32 consecutive cells and hands each cell's
-// right-face state to the next lane with a shuffle (31 faces per warp); along y
-// and z each thread marches over a segment of SEG faces and carries the previous
-// cell's state in registers.
+// through HBM.
+//  * x faces: the cells pos in [2, nx-2) of all rows form one flattened
+//    sequence; warp w takes cells [31w, 31w+32) of it, and each lane hands its
+//    cell's right-face state to the next lane with a shuffle (31 faces per warp,
+//    every lane busy whatever the row length).
+//  * y / z faces: one thread per column (x fastest, then the other transverse
+//    axis, flattened), marching along A over a segment of faces; the previous
+//    cell's right-face state waits in a shared-memory slot of the thread, not in
+//    registers, so the reconstruction and the Riemann solver do not hold it live.
+// Resident-block caps per Riemann solver: the reconstruction's 6 (80 registers),
+// Roe's 4 (its flux needs 128).
 // ---------------------------------------------------------------------------
 #ifndef QAS_SWEEP_MINB
-#define QAS_SWEEP_MINB 4
+#define QAS_SWEEP_MINB 6
 #endif
-#ifndef QAS_SWEEP_SEG
-#define QAS_SWEEP_SEG 16
+#ifndef QAS_SWEEP_ROE_MINB
+#define QAS_SWEEP_ROE_MINB 4
 #endif
+#define QAS_SWEEP_MINB_OF(RMN) ((RMN) == 0 ? QAS_SWEEP_ROE_MINB : QAS_SWEEP_MINB)
 
 template <int ODR, int A>
 __device__ __forceinline__ void cell_states(const View &v, long long c, double vl[7], double vr[7], double ql[2],
@@ -528,7 +555,6 @@ __device__ __forceinline__ void face_flux(const View &v, long long f, const doub
   const Geo &g = v.g;
   const long long s = g.s[A];
   constexpr int B = (A + 1) % 3, C = (A + 2) % 3;
-  double F[7];
   const double bnf = __ldg(v.u[4 + A] + f);
   const double bn = 0.5 * (bnf + bnf);
   double dv0 = 0.0, dv1 = 0.0;
@@ -543,76 +569,77 @@ __device__ __forceinline__ void face_flux(const View &v, long long f, const doub
       dv1 = qmin(qmin(__ldg(d1 + f - s), __ldg(d1 + f)), qmin(__ldg(d2 + f - s), __ldg(d2 + f)));
     }
   }
-  riemann<RMN>(L, R, bn, v.gam, dv0, dv1, F);
-  v.f[A][0][f] = F[0];
-  v.f[A][1 + A][f] = F[1];
-  v.f[A][1 + B][f] = F[2];
-  v.f[A][1 + C][f] = F[3];
-  double fbt = F[4], fbu = F[5];
-  if (g.dim >= 2) {
-    if (g.dim == 3 || A == 0) {
-      const double fc0 = 0.5 * (QL[0] + QR[0]);
-      v.fc[A][0][f] = fc0;
-      fbt -= fc0;
-    }
-    if (g.dim == 3 || A == 1) {
-      const double fc1 = 0.5 * (QL[1] + QR[1]);
-      v.fc[A][1][f] = fc1;
-      fbu -= fc1;
-    }
-  }
-  v.f[A][4 + B][f] = fbt;
-  v.f[A][4 + C][f] = fbu;
-  v.f[A][7][f] = v.phi ? F[6] + F[0] * 0.5 * (__ldg(v.phi + f - s) + __ldg(v.phi + f)) : F[6];
+  riemann_out<RMN>(L, R, bn, v.gam, dv0, dv1, FaceSink<A, false>{v, f, s, QL[0], QR[0], QL[1], QR[1], 0.0});
 }
 
-// x sweep: 4 warps per block, 31 faces per warp
+// x sweep: 4 warps per block, 31 faces per warp over the flattened cells of all rows
 template <int ODR, int RMN>
-__global__ void __launch_bounds__(128, QAS_SWEEP_MINB) k_sweep_x(View v)
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_x(View v, long long nwarps)
 {
   if (v.ctl->done) return;
   const Geo &g = v.g;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int f0 = 2 + (blockIdx.x * 4 + wid) * 31;  // cell of lane 0
-  const int i = f0 + lane;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const bool have_cell = i >= 2 && i < g.nx - 2;
+  const int lane = threadIdx.x & 31;
+  const long long w = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (w >= nwarps) return;  // the whole warp leaves together
+  const long long ncell = g.nx - 4;
+  const long long total = ncell * g.ny * g.nz;
+  long long t = w * 31 + lane;
+  const bool have_cell = t < total;
+  if (!have_cell) t = total - 1;  // a valid cell, computed and discarded (keeps the warp converged)
+  const long long row = t / ncell;
+  const int i = 2 + (int)(t - row * ncell);
+  const long long c = cidx(g, i, (int)(row % g.ny), (int)(row / g.ny));
   double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
-  const long long c = cidx(g, i < g.nx ? i : g.nx - 1, j, k);
-  if (have_cell) cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
+  cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
   double L[7], QL[2];
 #pragma unroll
   for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
   QL[0] = __shfl_up_sync(0xffffffffu, ql[0], 1);
   QL[1] = __shfl_up_sync(0xffffffffu, ql[1], 1);
-  if (lane >= 1 && i >= 3 && i < g.nx - 2) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
+  // lane-1 holds cell i-1 of the same row exactly when i >= 3
+  if (lane >= 1 && have_cell && i >= 3) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
 }
 
-// y / z sweep: each thread marches over SEG faces along A, threads along x
+// y / z sweep: one thread per column, marching over `seg` faces along A
 template <int ODR, int RMN, int A>
-__global__ void __launch_bounds__(128, QAS_SWEEP_MINB) k_sweep_m(View v)
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v, int seg)
 {
   if (v.ctl->done) return;
   const Geo &g = v.g;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.nx) return;
+  __shared__ double carry[9][128];  // previous cell's right-face state and induction state, per thread
+  const int tid = threadIdx.x;
+  const int no = A == 1 ? g.nz : g.ny;  // extent of the other transverse axis
+  const long long col = (long long)blockIdx.x * 128 + tid;
+  if (col >= (long long)g.nx * no) return;  // no barrier below: threads leave freely
+  const int i = (int)(col % g.nx), o = (int)(col / g.nx);
   const int n = g.n[A];
-  const int p0 = 3 + (A == 1 ? blockIdx.y : blockIdx.z) * QAS_SWEEP_SEG;
-  const int other = A == 1 ? blockIdx.z : blockIdx.y;  // k for the y sweep, j for the z sweep
-  const int p1 = min(p0 + QAS_SWEEP_SEG, n - 2);
+  const int p0 = 3 + blockIdx.y * seg;
+  const int p1 = min(p0 + seg, n - 2);
   const long long s = g.s[A];
-  long long c = A == 1 ? cidx(g, i, p0 - 1, other) : cidx(g, i, other, p0 - 1);
-  double L[7], QL[2] = {0.0, 0.0}, tmp[7], tq[2] = {0.0, 0.0};
-  cell_states<ODR, A>(v, c, L, tmp, QL, tq);
+  long long c = A == 1 ? cidx(g, i, p0 - 1, o) : cidx(g, i, o, p0 - 1);
+  {
+    double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+    cell_states<ODR, A>(v, c, vl, vr, ql, qr);
+#pragma unroll
+    for (int m = 0; m < 7; m++) carry[m][tid] = vl[m];
+    carry[7][tid] = ql[0];
+    carry[8][tid] = ql[1];
+  }
   for (int p = p0; p < p1; p++) {
     c += s;
     double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
     cell_states<ODR, A>(v, c, vl, vr, ql, qr);
-    face_flux<RMN, A>(v, c, L, vr, QL, qr);
+    double L[7], QL[2];
 #pragma unroll
-    for (int m = 0; m < 7; m++) L[m] = vl[m];
-    QL[0] = ql[0];
-    QL[1] = ql[1];
+    for (int m = 0; m < 7; m++) {
+      L[m] = carry[m][tid];
+      carry[m][tid] = vl[m];
+    }
+    QL[0] = carry[7][tid];
+    QL[1] = carry[8][tid];
+    carry[7][tid] = ql[0];
+    carry[8][tid] = ql[1];
+    face_flux<RMN, A>(v, c, L, vr, QL, qr);
   }
 }
 

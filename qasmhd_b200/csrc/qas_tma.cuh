@@ -10,9 +10,9 @@
 //   * A == 0 (x faces): each plane is an x-tile with a +-2 halo, streamed along MA.
 // One elected thread issues the loads of the next plane while all threads compute the
 // current cell; the arithmetic is lr_cell, the same function as the global-memory k_lr, so
-// the results are bit-identical.  Every mbarrier wait is bounded (about two seconds of
-// device time): on expiry the kernel latches an error bit, waits (bounded) for its own loads
-// in flight and returns.
+// the results are bit-identical.  Every mbarrier wait is bounded (two seconds of device time
+// by %globaltimer, LrTmaPlan::wait_ns): on expiry the kernel latches an error bit, waits
+// (bounded) for its own loads in flight and returns.
 #pragma once
 
 #include <cuda.h>
@@ -34,6 +34,11 @@ struct LrTmaPlan {
   int mlo, mhi;    // computed range along the march axis
   int xlo, xhi;    // computed range along x
   int nr;          // extent of the row axis
+  // bound of every mbarrier wait in ns of device time (2 s), and a failure hook for tests: when
+  // stall_plane >= 0, no CTA issues its plane number stall_plane (counted from the CTA's first),
+  // so the wait for that plane runs out and the kernel takes its timeout path
+  unsigned long long wait_ns;
+  int stall_plane;
 };
 
 constexpr int LR_TMA_TIMEOUT_BIT = 8;
@@ -71,13 +76,14 @@ __device__ __forceinline__ unsigned long long global_ns()
   return t;
 }
 
-// wait for phase `parity` of the barrier, giving up after ~2 s of device time
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity)
+// wait for phase `parity` of the barrier, giving up after `limit_ns` of device time
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity,
+                                                  unsigned long long limit_ns)
 {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -163,6 +169,7 @@ __global__ void __launch_bounds__(TX *TR, 5) k_lr_tma(View v, const __grid_const
       const int slot = (int)(gq % S::R);
       const int m = m0 - S::H + q;
       const int cy = MA == 1 ? m : r0, cz = MA == 1 ? r0 : m;
+      if ((int)gq == pl.stall_plane) return;  // test hook: this plane is never loaded
       mbar_arrive_expect_tx(&bar[slot], S::PLANE_BYTES);
 #pragma unroll
       for (int f = 0; f < NF; f++) tma_load_3d(lr_ring + (slot * NF + f) * S::PD, &maps.m[f], bx0, cy, cz, &bar[slot]);
@@ -179,7 +186,7 @@ __global__ void __launch_bounds__(TX *TR, 5) k_lr_tma(View v, const __grid_const
     for (int s = 0; s < ns; s++) {
       for (int q = waited; q <= s + S::W - 1; q++) {
         const unsigned gq = gbase + q;
-        if (!mbar_wait_bounded(&bar[gq % S::R], (gq / S::R) & 1)) timeout = 1;
+        if (!mbar_wait_bounded(&bar[gq % S::R], (gq / S::R) & 1, pl.wait_ns)) timeout = 1;
       }
       waited = s + S::W;
       if (!timeout && live) {
@@ -194,7 +201,7 @@ __global__ void __launch_bounds__(TX *TR, 5) k_lr_tma(View v, const __grid_const
           atomicOr(&v.ctl->err, LR_TMA_TIMEOUT_BIT);
           for (int q = waited; q < issued; q++) {  // own loads still in flight
             const unsigned gq = gbase + q;
-            mbar_wait_bounded(&bar[gq % S::R], (gq / S::R) & 1);
+            mbar_wait_bounded(&bar[gq % S::R], (gq / S::R) & 1, pl.wait_ns);
           }
         }
         __syncthreads();

@@ -46,6 +46,7 @@ QAS_OPT_FUSED_SWEEP = 1
 QAS_OPT_LR_STAGING = 2
 QAS_OPT_PIPE_ITEMS = 3
 QAS_OPT_PIPE_LANES = 4
+QAS_OPT_TEST_TMA_STALL = 5
 
 
 class QasError(RuntimeError):

@@ -65,11 +65,21 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
         return a
     if kind == "cuct":
         return np.concatenate([np.abs(rng.normal(1, 0.2, (n, 4))) + 0.1, rng.normal(0, 1, (n, 16))], axis=1)
+    if kind == "energy":
+        # ro, vx, vy, vz, bx, by, bz, pr-or-en, gamma: low-Mach rows (kinetic energy ~1e-8 of the
+        # pressure's), exact zeros and the benchmark gammas
+        a = np.column_stack([np.abs(rng.normal(1, 0.3, n)) + 0.05, rng.normal(0, 1, (n, 6)),
+                             np.abs(rng.normal(1, 0.5, n)) + 0.05,
+                             rng.choice([5.0 / 3.0, 2.0, 1.4], n)])
+        a[::5, 1:4] *= 1e-4
+        a[2::9, 2:4] = 0.0
+        a[4::11, 5:7] = 0.0
+        return a
     raise ValueError(kind)
 
 
 KAT_FUNCS = {"flux": ([0, 1, 2, 3], 7), "interp": (list(range(10, 20)), 2), "lrstate": ([20, 21, 22, 23], 14),
-             "lrstate_prim": ([24, 25, 26, 27], 14), "cuct": ([30], 1)}
+             "lrstate_prim": ([24, 25, 26, 27], 14), "cuct": ([30], 1), "energy": ([31, 32], 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -148,7 +158,19 @@ def make_kat_prim() -> None:
     print("kat lrstate_prim", inp.shape)
 
 
+def make_kat(name: str) -> None:
+    """One point-function fixture, kat_<name>.npz."""
+    funcs, nout = KAT_FUNCS[name]
+    inp = kat_inputs(name)
+    outs = {f"f{f}": R.run_kat(f, inp, nout) for f in funcs}
+    np.savez_compressed(os.path.join(OUT, f"kat_{name}.npz"), input_sha=sha(inp), **outs)
+    print("kat", name, inp.shape)
+
+
 def main() -> None:
+    if len(sys.argv) > 2 and sys.argv[1] == "--kat":  # one fixture only
+        make_kat(sys.argv[2])
+        return
     for name, (funcs, nout) in KAT_FUNCS.items():
         if name == "lrstate_prim":
             continue
