@@ -89,8 +89,8 @@ struct qas_ctx {
   qas_status latched = QAS_OK;
   // thread-block tile (x,y,z extents, 128 threads) of every cell kernel, by kernel id
   dim3 tile[32];
-  // face sweep form: two kernels with the face states in HBM (default, measured faster on
-  // B200: both halves are latency/FP64-bound, the fused kernel spills) or one fused kernel
+  // face sweep form: two kernels with the face states in HBM, or one fused kernel (the
+  // default in 3D, set at creation)
   bool fused = false;
   int sweep_seg[3] = {0, 0, 0};  // segment length of the fused y / z sweeps (0: not chosen yet)
   // live per-kernel timing (qas_profile_run): an event pair around every launch
@@ -982,6 +982,12 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   // by FP64 dependency latency, and the staged form measured 9-35 % slower per launch
   c->lr_tma_ok = scheme->odr == 4 && setup_lr_tma(c);
   c->lr_tma = false;
+  // face sweep form: fused (face states never in HBM) in 3D, where it measured faster on B200
+  // (KH 256^3, MLAU: 2.78 ms per sweep against 1.90 + 1.21 ms for the two kernels, and a cooler
+  // step under the power cap); two kernels in 1D/2D, where the y sweep has too few columns to
+  // march long segments (OT 1024^2: 0.164 against 0.102 + 0.050 ms)
+  c->fused = g.dim == 3;
+  if (c->fused) sweep_prepare(c);
   if (cudaMemsetAsync(c->d_dctl, 0, sizeof(DCtl), c->stream) != cudaSuccess) return fail(QAS_ERR_CUDA);
   if ((st = write_ctl(c)) != QAS_OK) return fail(st);
   *out = c;

@@ -1,11 +1,13 @@
 """Bit-exact parity at the benchmark sizes.
 
 * C1, Brio-Wu 1024 to t = 0.1 (961 exec_ steps): against the oracle, run live.
-* C2, Orszag-Tang 1024^2 to t = 0.5 and C3, Kelvin-Helmholtz 256^3 for 20 steps: the reference
-  build's own final states are too large to commit, so tests/golden/fullsize.json holds their
-  SHA-256 fingerprints (made by tests/golden/make_fullsize.py from oracle/_ref), and the GPU's
-  final state must hash to the same value -- through the device-resident exec_ loop and, for
-  C2, through ~600 host round trips of qas_step_host."""
+* C2, Orszag-Tang 1024^2 to t = 0.5, C3, Kelvin-Helmholtz 256^3 for 20 steps and at 64^3 for
+  its full 1000 steps, and sampled C4 ensemble members (64..512 per side, both halves, the
+  Mach / beta extremes) for their 200 steps in one batch: the reference build's own final
+  states are too large to commit, so tests/golden/fullsize.json holds their SHA-256
+  fingerprints (made by tests/golden/make_fullsize.py from oracle/_ref), and the GPU's final
+  state must hash to the same value -- through the device-resident exec_ loop, the batched
+  ensemble and, for C2, through ~600 host round trips of qas_step_host."""
 import hashlib
 import json
 import os
@@ -75,3 +77,26 @@ def test_c3_kelvin_helmholtz_256_20_steps():
     b = run_gpu(p, R.MODE_RUN, nsteps=20)
     assert b["steps"] == 20 and b["dt"] == g["dt"]
     assert fingerprint(b["state"]) == g["sha256"]
+
+
+def test_c3_kelvin_helmholtz_64_full_1000_steps():
+    g = golden("kh3d_64_1000steps")
+    p = P.kelvin_helmholtz(3, 64)
+    b = run_gpu(p, R.MODE_RUN, nsteps=1000)
+    assert b["steps"] == 1000 and b["dt"] == g["dt"] and b["tim"] == g["tim"]
+    assert fingerprint(b["state"]) == g["sha256"]
+
+
+def test_c4_sampled_instances_200_steps_batched():
+    from tests.golden.make_fullsize import C4_SAMPLE, C4_STEPS
+    gold = [golden(f"c4_{q}") for q in C4_SAMPLE]
+    ens = P.ensemble(512)
+    probs = [ens[q] for q in C4_SAMPLE]
+    with L.Batch(probs) as b:
+        for i, p in enumerate(probs):
+            b.upload(i, p.state)
+        info = b.run(max_steps=C4_STEPS, flg=1, stop_rule=0, cfl=0.4)
+        outs = [b.download(i, p.state.shape) for i, p in enumerate(probs)]
+    for i, q in enumerate(C4_SAMPLE):
+        assert info[i][0] == C4_STEPS and info[i][2] == gold[i]["dt"], (q, info[i], gold[i])
+        assert fingerprint(outs[i]) == gold[i]["sha256"], f"ensemble member {q} ({probs[i].name})"

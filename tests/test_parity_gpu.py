@@ -197,17 +197,21 @@ def test_kh_256_determinism_and_divb():
     assert d < 1e-10, d
 
 
-@pytest.mark.parametrize("dim,rmn", [(1, 1), (2, 1), (2, 3), (3, 0), (3, 3)])
-def test_fused_sweep_form(restatement, dim, rmn):
-    p = {1: lambda: P.brio_wu(96, rmn=rmn), 2: lambda: P.orszag_tang(48, rmn=rmn),
-         3: lambda: P.kelvin_helmholtz(3, 12, mach=0.3, rmn=rmn)}[dim]()
+@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("dim,rmn", [(1, 1), (2, 1), (2, 3), (3, 0), (3, 1), (3, 2), (3, 3)])
+def test_sweep_forms(restatement, dim, rmn, fused):
+    """Both face-sweep forms (two kernels, or one fused kernel: the 3D default) against the
+    oracle; odd extents and a non-cubic 3D box exercise the flattened x warps and the y / z
+    segment ends."""
+    p = {1: lambda: P.brio_wu(96, rmn=rmn), 2: lambda: P.orszag_tang(48, nym=37, rmn=rmn),
+         3: lambda: P.kelvin_helmholtz(3, 12, nym=9, nzm=15, mach=0.3, rmn=rmn)}[dim]()
     a = restatement.run(p, 3, mode=R.MODE_RUN)
     with L.Context.from_problem(p) as ctx:
-        ctx.set_option(L.QAS_OPT_FUSED_SWEEP, 1)
+        ctx.set_option(L.QAS_OPT_FUSED_SWEEP, fused)
         ctx.upload(p.state)
         ctx.run(max_steps=3, flg=p.flg, stop_rule=0, cfl=p.cfl)
         out = ctx.download(p.state.shape)
-    assert_bitwise(out, a["state"], f"fused dim{dim} rmn{rmn}")
+    assert_bitwise(out, a["state"], f"fused={fused} dim{dim} rmn{rmn}")
 
 
 def test_profile_run_reports_kernels():
