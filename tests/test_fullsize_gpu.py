@@ -33,7 +33,10 @@ def golden(key):
     if not os.path.exists(GOLDEN):
         pytest.skip("tests/golden/fullsize.json not generated")
     with open(GOLDEN) as f:
-        return json.load(f)[key]
+        data = json.load(f)
+    if key not in data:
+        pytest.skip(f"{key} not in tests/golden/fullsize.json (tests/golden/make_fullsize.py {key})")
+    return data[key]
 
 
 def test_c1_brio_wu_full_run(restatement):
