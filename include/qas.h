@@ -61,8 +61,10 @@ typedef struct {
  *   char_mode: face-value reconstruction of mhd_lrstate (common/mhd_func.c:108-161): 0 in
  *     characteristic variables with the mhd_eigen_mi/ae eigenvectors (the reference's active
  *     code, default); 1 in primitive variables, each field on its own (mhd_reconst,
- *     common/mhd_eigen.c:667-706, the reference's debug alternative).  Appended field: a
- *     zero-initialised struct keeps the default. */
+ *     common/mhd_eigen.c:667-706, the reference's debug alternative); 2 in characteristic
+ *     variables with the Athena-type eigenvectors of mhd_eigen_st for every state (mhd_c_reconst,
+ *     common/mhd_eigen.c:5-173,436-511, the reference's third option).  Appended field: a
+ *     zero-initialised struct keeps the default.  The adjoint takes 0 only. */
 typedef struct {
   int rmn, odr, rk, ctw;
   int char_mode;

@@ -263,14 +263,81 @@ static void eig_alfven_entropy(double ro, double bx, double by, double bz, doubl
   R[6][3] = +isroh; R[6][5] = -0.5; R[6][6] = +bzh;
 }
 
-/* characteristic reconstruction: common/mhd_eigen.c:513-665.
+/* Athena-type eigenvectors of the non-conservative form: mhd_eigen_st (common/mhd_eigen.c:5-173);
+ * L[k] = row l(k+1), R[k] = column r(k+1) */
+static void eig_athena(double ro, double bx, double by, double bz, double pr, double gamma,
+                       double L[7][7], double R[7][7])
+{
+  double eps = 1e-12;
+  double sqrt2 = sqrt(2.0);
+  double iro = 1.0 / ro;
+  double sro = sqrt(ro);
+  double isro = 1.0 / sro;
+  double bxsr = bx * isro, bysr = by * isro, bzsr = bz * isro;
+  double bx2 = bxsr * bxsr;
+  double bt2 = bysr * bysr + bzsr * bzsr;
+  double b2 = bx2 + bt2;
+  double a2 = fabs(gamma * pr / ro);
+  double aa = sqrt(a2);
+  double ca2 = bx2;
+  double junk = sqrt(fabs((a2 + b2) * (a2 + b2) - 4.0 * a2 * ca2));
+  double cf2 = fabs(0.5 * (a2 + b2 + junk));
+  double cf = sqrt(cf2);
+  double cs2 = fabs(0.5 * (a2 + b2 - junk));
+  double cs = sqrt(cs2);
+  bx2 = bx * bx;
+  bt2 = by * by + bz * bz;
+  b2 = bx2 + bt2;
+  double denom = 1.0 / sqrt(bt2);
+  int flag = (bt2 > eps * b2);
+  double betay = (flag) ? (by * denom) : (0.5 * sqrt2);
+  double betaz = (flag) ? (bz * denom) : (0.5 * sqrt2);
+  denom = 1.0 / sqrt(fabs(cf2 - cs2));
+  flag = ((bt2 > eps * b2) || (fabs(gamma * pr - bx2) > eps * gamma * pr));
+  double alphaf = (flag) ? (sqrt(fabs(a2 - cs2)) * denom) : 1.0;
+  double alphas = (flag) ? (sqrt(fabs(cf2 - a2)) * denom) : 0.0;
+  double sgnbx = (bx > 0) ? (1.0) : (-1.0);
+  double cfalf = cf * alphaf, csals = cs * alphas, aaalf = aa * alphaf, aaals = aa * alphas;
+  int n;
+  denom = 0.5 / a2;
+  memset(L, 0, sizeof(double) * 49);
+  memset(R, 0, sizeof(double) * 49);
+  L[0][1] = -cfalf * denom; L[0][2] = +csals * denom * sgnbx * betay; L[0][3] = +csals * denom * sgnbx * betaz;
+  L[0][4] = +aaals * denom * isro * betay; L[0][5] = +aaals * denom * isro * betaz; L[0][6] = alphaf * denom * iro;
+  L[1][2] = -0.5 * betaz; L[1][3] = +0.5 * betay;
+  L[1][4] = -0.5 * isro * betaz * sgnbx; L[1][5] = +0.5 * isro * betay * sgnbx;
+  L[2][1] = -csals * denom; L[2][2] = -cfalf * denom * sgnbx * betay; L[2][3] = -cfalf * denom * sgnbx * betaz;
+  L[2][4] = -aaalf * denom * isro * betay; L[2][5] = -aaalf * denom * isro * betaz; L[2][6] = alphas * denom * iro;
+  L[3][0] = 1.0; L[3][6] = -1.0 / a2;
+  R[0][0] = ro * alphaf; R[0][1] = -cfalf; R[0][2] = +csals * sgnbx * betay; R[0][3] = +csals * sgnbx * betaz;
+  R[0][4] = +aaals * sro * betay; R[0][5] = +aaals * sro * betaz; R[0][6] = alphaf * gamma * pr;
+  R[1][2] = -betaz; R[1][3] = +betay; R[1][4] = -sro * betaz * sgnbx; R[1][5] = +sro * betay * sgnbx;
+  R[2][0] = ro * alphas; R[2][1] = -csals; R[2][2] = -cfalf * sgnbx * betay; R[2][3] = -cfalf * sgnbx * betaz;
+  R[2][4] = -aaalf * sro * betay; R[2][5] = -aaalf * sro * betaz; R[2][6] = alphas * gamma * pr;
+  R[3][0] = 1.0;
+  /* l7, l6, l5 (r7, r6, r5) mirror l1, l2, l3: +, -, -, -, +, +, + */
+  for (n = 0; n < 7; n++) {
+    const double sg = (n >= 1 && n <= 3) ? -1.0 : 1.0;
+    L[6][n] = sg > 0 ? +L[0][n] : -L[0][n];
+    L[5][n] = sg > 0 ? +L[1][n] : -L[1][n];
+    L[4][n] = sg > 0 ? +L[2][n] : -L[2][n];
+    R[6][n] = sg > 0 ? +R[0][n] : -R[0][n];
+    R[5][n] = sg > 0 ? +R[1][n] : -R[1][n];
+    R[4][n] = sg > 0 ? +R[2][n] : -R[2][n];
+  }
+}
+
+/* characteristic reconstruction: common/mhd_eigen.c:513-665 (mode 0: mhd_m_reconst's
+ * eigenvectors when fast, mhd_a_reconst's else) and :436-511 (mode 2: mhd_c_reconst).
  * q[v][m]: primitive v (ro,vn,vt,vu,bt,bu,pr) at stencil point m=0..4 */
-static void char_reconst(int fast, const double q[7][5], double bn, double gamma, lr_fn lr,
+static void char_reconst(int fast, int mode, const double q[7][5], double bn, double gamma, lr_fn lr,
                          double *ul, double *ur)
 {
   double L[7][7], R[7][7], w[7][5], wl[7], wr[7];
   int k, m, n;
-  if (fast)
+  if (mode == 2)
+    eig_athena(q[0][2], bn, q[4][2], q[5][2], q[6][2], gamma, L, R);
+  else if (fast)
     eig_fast_alfven(q[0][2], bn, q[4][2], q[5][2], q[6][2], gamma, L, R);
   else
     eig_alfven_entropy(q[0][2], bn, q[4][2], q[5][2], q[6][2], gamma, L, R);
@@ -296,17 +363,17 @@ static void char_reconst(int fast, const double q[7][5], double bn, double gamma
   }
 }
 
-/* face states: common/mhd_func.c:108-161 */
-/* mhd_lrstate (common/mhd_func.c:108-161); prim: the reconstruction call replaced by the
- * primitive-variable mhd_reconst (common/mhd_eigen.c:667-706) */
-static void face_states(const double q[7][5], double bn, double gamma, lr_fn lr, double *vl, double *vr, int prim)
+/* mhd_lrstate (common/mhd_func.c:108-161); mode 1: the reconstruction call replaced by the
+ * primitive-variable mhd_reconst (common/mhd_eigen.c:667-706), mode 2: by the Athena-type
+ * mhd_c_reconst (:436-511) */
+static void face_states(const double q[7][5], double bn, double gamma, lr_fn lr, double *vl, double *vr, int mode)
 {
   const double eps = 1e-12;
-  if (prim) {
+  if (mode == 1) {
     for (int n = 0; n < 7; n++) lr(&q[n][2], &vl[n], &vr[n]);
   } else {
     int fast = (q[0][2] * (q[1][2] * q[1][2] + q[2][2] * q[2][2] + q[3][2] * q[3][2]) > gamma * q[6][2]);
-    char_reconst(fast, q, bn, gamma, lr, vl, vr);
+    char_reconst(fast, mode, q, bn, gamma, lr, vl, vr);
   }
   if (vl[0] <= eps || vl[6] <= eps) {
     vl[0] = q[0][2];
@@ -1975,12 +2042,14 @@ int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out
       riemann(func)(&a[0], &a[7], a[14], a[15], &a[16], o);
     } else if (func >= 10 && func <= 19) {
       lrs[func - 10](&a[2], &o[0], &o[1]);
-    } else if (func >= 20 && func <= 27) {  /* 24..27: with the primitive reconstruction */
+    } else if ((func >= 20 && func <= 27) || (func >= 40 && func <= 43)) {
+      /* 24..27: primitive reconstruction, 40..43: Athena-type */
       double q[7][5];
-      const int prim = func >= 24;
+      const int mode = func >= 40 ? 2 : (func >= 24 ? 1 : 0);
+      const int odr = func >= 40 ? func - 39 : (func >= 24 ? func - 23 : func - 19);
       for (int v = 0; v < 7; v++)
         for (int m = 0; m < 5; m++) q[v][m] = a[5 * v + m];
-      face_states(q, a[35], a[36], nl_interp(func - (prim ? 23 : 19)), &o[0], &o[7], prim);
+      face_states(q, a[35], a[36], nl_interp(odr), &o[0], &o[7], mode);
     } else if (func == 30) {
       o[0] = cuct_weight(&a[3], &a[7], &a[11], &a[15], &a[19], 1, 2);
     } else if (func == 31) {

@@ -31,7 +31,8 @@ typedef struct {
                           the by/bz fluxes of ideal() and hall_() get the crcte correction */
   const double *nu, *eta;  /* per-cell viscosity / resistivity of the dissipative drivers (the
                               API's nu/eta, nd doubles each); NULL: uniform nu0/eta0 arguments */
-  int char_mode;       /* 0 characteristic reconstruction (mhd_m/a_reconst), 1 primitive (mhd_reconst) */
+  int char_mode;       /* 0 characteristic reconstruction (mhd_m/a_reconst), 1 primitive (mhd_reconst),
+                          2 Athena-type characteristic (mhd_c_reconst) */
 } qo_grid;
 
 /* Ghost fill of the 8 state fields (bound(): mhd1d_class.cpp:3-9, mhd2d_class.cpp:3-9,
@@ -67,7 +68,8 @@ double qo_haldt(const qo_grid *g, const double *u, double cfl, double di, double
 
 /* Point-function known answers; same function ids and layouts as oracle/ref_harness/ref_kat.cpp,
  * plus 24..27: mhd_lrstate at ODR 1..4 with the primitive reconstruction mhd_reconst (the ids
- * 20..23 of the harness built against it, oracle/_ref/ref_kat_prim). */
+ * 20..23 of the harness built against it, oracle/_ref/ref_kat_prim), and 40..43: the same with
+ * the Athena-type reconstruction mhd_c_reconst (oracle/_ref/ref_kat_char). */
 int qo_kat(int func, int ncase, int nin, int nout, const double *in, double *out);
 
 #ifdef __cplusplus

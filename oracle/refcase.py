@@ -40,10 +40,11 @@ MAGIC_OUT = 0x32534151
 def ref_binary(dim: int, ctw: int, gravity=False) -> str:
     """The reference build for a case: ref1d, ref{2,3}d_ctw*, the gravity drivers
     (2D/SERIAL/RTI, 3D/MPI/RTI) ref{2,3}d_g_ctw* (gravity=True), the Hall driver ref1d_hall
-    (gravity="hall"), or the primitive-reconstruction builds ref1d_prim / ref{2,3}d_prim_ctw1
-    (gravity="prim")."""
-    if gravity == "prim":
-        name = "ref1d_prim" if dim == 1 else f"ref{dim}d_prim_ctw{int(bool(ctw))}"
+    (gravity="hall"), the primitive-reconstruction builds ref1d_prim / ref{2,3}d_prim_ctw1
+    (gravity="prim") or the Athena-type reconstruction builds ref1d_char / ref{2,3}d_char_ctw1
+    (gravity="char")."""
+    if gravity in ("prim", "char"):
+        name = f"ref1d_{gravity}" if dim == 1 else f"ref{dim}d_{gravity}_ctw{int(bool(ctw))}"
     elif dim == 1:
         name = "ref1d_hall" if gravity == "hall" else "ref1d"
     else:
@@ -151,7 +152,7 @@ def run_reference(prob, mode: int = MODE_RUN, nsteps: int = 1, dt: float = 0.0, 
     build of the same driver, e.g. o3_binary(), for timing; ``bind``: pin the OpenMP threads
     to consecutive cores, OMP_PROC_BIND=close OMP_PLACES=cores)."""
     if getattr(prob, "char_mode", 0):
-        variant = "prim"
+        variant = "prim" if prob.char_mode == 1 else "char"
     elif getattr(prob, "hall", False):
         variant = "hall"
     else:

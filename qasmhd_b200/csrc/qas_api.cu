@@ -448,10 +448,16 @@ void launch_lr(qas_ctx *c, int a)
     return;
   }
   const dim3 grid = cells_grid(c->geo, c->tile[KID_LR]), blk = c->tile[KID_LR];
-  if (c->view.recon) {
+  if (c->view.recon == 1) {
     if (a == 0) QL(c, KID_LR, k_lr<ODR, 0, 1><<<grid, blk, 0, c->stream>>>(c->view));
     if (a == 1) QL(c, KID_LR, k_lr<ODR, 1, 1><<<grid, blk, 0, c->stream>>>(c->view));
     if (a == 2) QL(c, KID_LR, k_lr<ODR, 2, 1><<<grid, blk, 0, c->stream>>>(c->view));
+    return;
+  }
+  if (c->view.recon == 2) {
+    if (a == 0) QL(c, KID_LR, k_lr<ODR, 0, 2><<<grid, blk, 0, c->stream>>>(c->view));
+    if (a == 1) QL(c, KID_LR, k_lr<ODR, 1, 2><<<grid, blk, 0, c->stream>>>(c->view));
+    if (a == 2) QL(c, KID_LR, k_lr<ODR, 2, 2><<<grid, blk, 0, c->stream>>>(c->view));
     return;
   }
   if (a == 0) QL(c, KID_LR, k_lr<ODR, 0><<<grid, blk, 0, c->stream>>>(c->view));
@@ -503,10 +509,25 @@ int sweep_seg(qas_ctx *c, int a, const void *fn)
   return bseg;
 }
 
+// shared-memory carveout hint of the fused sweeps (percent of the SM's maximum; -1: the driver's
+// choice): the y / z sweeps read each stencil plane five times along their march, from L1
+// when the rest of the SM's 256 KB is left to it
+#ifndef QAS_SWEEP_CARVEOUT
+#define QAS_SWEEP_CARVEOUT -1
+#endif
 // choose the y / z segment lengths outside any stream capture (occupancy query)
 template <int ODR, int RMN>
 void sweep_prepare_t(qas_ctx *c)
 {
+  if (QAS_SWEEP_CARVEOUT >= 0) {
+    cudaFuncSetAttribute((const void *)k_sweep_x<ODR, RMN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         QAS_SWEEP_CARVEOUT);
+    cudaFuncSetAttribute((const void *)k_sweep_m<ODR, RMN, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         QAS_SWEEP_CARVEOUT);
+    cudaFuncSetAttribute((const void *)k_sweep_m<ODR, RMN, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         QAS_SWEEP_CARVEOUT);
+    cudaGetLastError();
+  }
   if (c->geo.dim >= 2) sweep_seg(c, 1, (const void *)k_sweep_m<ODR, RMN, 1>);
   if (c->geo.dim >= 3) sweep_seg(c, 2, (const void *)k_sweep_m<ODR, RMN, 2>);
 }
@@ -883,7 +904,7 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   if (gr.dim >= 3 && gr.nzm < 4) return QAS_ERR_INVALID;
   if (!(gr.dx > 0) || (gr.dim >= 2 && !(gr.dy > 0)) || (gr.dim >= 3 && !(gr.dz > 0))) return QAS_ERR_INVALID;
   if (scheme->rmn < 0 || scheme->rmn > 3 || scheme->odr < 1 || scheme->odr > 4 || scheme->rk < 1 ||
-      scheme->rk > 3 || scheme->char_mode < 0 || scheme->char_mode > 1)
+      scheme->rk > 3 || scheme->char_mode < 0 || scheme->char_mode > 2)
     return QAS_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return QAS_ERR_NO_DEVICE;

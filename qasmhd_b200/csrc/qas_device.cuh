@@ -11,6 +11,13 @@
 #pragma once
 
 #include <math.h>
+
+#ifndef QAS_ZERO_INT
+#define QAS_ZERO_INT 0
+#endif
+#ifndef QAS_WCNS4_NOINLINE
+#define QAS_WCNS4_NOINLINE 0
+#endif
 #if defined(__CUDACC__)
 #include <cuda_runtime.h>
 #define QAS_HD __host__ __device__ __forceinline__
@@ -23,6 +30,18 @@ namespace qas {
 // ---------------------------------------------------------------------------
 // common/common_func.h:4-31
 // ---------------------------------------------------------------------------
+// exact-zero test of the reconstruction's zero-preservation flags (x == 0.0, both signs); on
+// the device with QAS_ZERO_INT as an integer test of the bits, which keeps it off the FP64 pipe
+// (same truth value for every input, NaN included)
+QAS_HD bool is_zero(double x)
+{
+#if defined(__CUDA_ARCH__) && QAS_ZERO_INT
+  return (__double_as_longlong(x) << 1) == 0;
+#else
+  return x == 0.0;
+#endif
+}
+
 QAS_HD double qmax(double a, double b) { return (a >= b) ? a : b; }
 QAS_HD double qmin(double a, double b) { return (a >= b) ? b : a; }
 QAS_HD double minmod(double a, double b)
@@ -88,7 +107,13 @@ QAS_HD double lin_right(const double f[5])
 // 1st order, MUSCL minmod (common_interp.c:32-37), WCNS3 (:65-101),
 // WCNS4 (:102-150)
 // ---------------------------------------------------------------------------
+// QAS_WCNS4_NOINLINE: one out-of-line copy of the WCNS4 interpolation on the device instead of
+// one per characteristic field (smaller kernels, fewer instruction-cache misses)
+#if defined(__CUDACC__) && QAS_WCNS4_NOINLINE
+__host__ __device__ __noinline__ void wcns4_lr(const double f[5], double &fl, double &fr)
+#else
 QAS_HD void wcns4_lr(const double f[5], double &fl, double &fr)
+#endif
 {
   const double eps = 1e-40;
   double c1, c2;
@@ -333,9 +358,9 @@ QAS_HD void face_states_grouped(const Stencil &P, double bn, double gam, double 
 #pragma unroll
     for (int m = 0; m < 5; m++) {
       const double r_ = P(0, m), n_ = P(1, m), b_ = P(4, m), c_ = P(5, m), p_ = P(6, m);
-      zvn = zvn && (n_ == 0.0);
-      zbt = zbt && (b_ == 0.0);
-      zbu = zbu && (c_ == 0.0);
+      zvn = zvn && is_zero(n_);
+      zbt = zbt && is_zero(b_);
+      zbu = zbu && is_zero(c_);
       w0[m] = fast ? (((nrcf * n_ + by * b_) + bz * c_) + p_) : n_;
       w1[m] = ((cf2 * r_ - by * b_) - bz * c_) - p_;
       w2[m] = fast ? (((rcf * n_ + by * b_) + bz * c_) + p_) : ((by * b_ + bz * c_) + p_);
@@ -349,7 +374,7 @@ QAS_HD void face_states_grouped(const Stencil &P, double bn, double gam, double 
 #pragma unroll
     for (int m = 0; m < 5; m++) {
       const double t_ = P(2, m), b_ = P(4, m);
-      zvt = zvt && (t_ == 0.0);
+      zvt = zvt && is_zero(t_);
       w3[m] = sro * t_ + b_;
       w4[m] = sro * t_ - b_;
     }
@@ -361,7 +386,7 @@ QAS_HD void face_states_grouped(const Stencil &P, double bn, double gam, double 
 #pragma unroll
     for (int m = 0; m < 5; m++) {
       const double u_ = P(3, m), c_ = P(5, m);
-      zvu = zvu && (u_ == 0.0);
+      zvu = zvu && is_zero(u_);
       w5[m] = sro * u_ + c_;
       w6[m] = sro * u_ - c_;
     }
@@ -403,6 +428,135 @@ QAS_HD void face_states_grouped(const Stencil &P, double bn, double gam, double 
     vl[6] = pr;
   }
   if (vr[0] <= eps || vr[6] <= eps) {
+    vr[0] = ro;
+    vr[1] = vn;
+    vr[6] = pr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// mhd_lrstate with the Athena-type characteristic reconstruction mhd_c_reconst
+// (common/mhd_eigen.c:436-511) and the eigenvectors of mhd_eigen_st (:5-173, Stone et al.
+// 2008, ApJS 178, 137), which the reference offers beside mhd_m/a_reconst (the call in
+// mhd_lrstate switched): one eigen-system for every state, no fast/slow choice.  L and R are
+// 7x7 with literal zeros; each projection keeps the reference's left-to-right sum over the
+// non-zero entries (an omitted 0*x term can only change the sign of an exact zero), every
+// entry formed by the reference's expression.  Then the exact-zero flags of mhd_c_reconst and
+// the positivity fallback of mhd_lrstate.
+// ---------------------------------------------------------------------------
+template <int ODR, class Stencil>
+QAS_HD void face_states_athena(const Stencil &P, double bx, double gamma, double vl[7], double vr[7])
+{
+  const double ro = P(0, 2), vn = P(1, 2), by = P(4, 2), bz = P(5, 2), pr = P(6, 2);
+  // mhd_eigen_st at the centre point
+  const double eps = 1e-12;
+  const double sqrt2 = sqrt(2.0);
+  double iro = 1.0 / ro;
+  double sro = sqrt(ro);
+  double isro = 1.0 / sro;
+  double bxsr = bx * isro;
+  double bysr = by * isro;
+  double bzsr = bz * isro;
+  double bx2 = bxsr * bxsr;
+  double bt2 = bysr * bysr + bzsr * bzsr;
+  double b2 = bx2 + bt2;
+  double a2 = fabs(gamma * pr / ro);
+  double aa = sqrt(a2);
+  double ca2 = bx2;
+  double junk = sqrt(fabs((a2 + b2) * (a2 + b2) - 4.0 * a2 * ca2));
+  double cf2 = fabs(0.5 * (a2 + b2 + junk));
+  double cf = sqrt(cf2);
+  double cs2 = fabs(0.5 * (a2 + b2 - junk));
+  double cs = sqrt(cs2);
+  bx2 = bx * bx;
+  bt2 = by * by + bz * bz;
+  b2 = bx2 + bt2;
+  double denom = 1.0 / sqrt(bt2);
+  bool flag = (bt2 > eps * b2);
+  const double betay = flag ? (by * denom) : (0.5 * sqrt2);
+  const double betaz = flag ? (bz * denom) : (0.5 * sqrt2);
+  denom = 1.0 / sqrt(fabs(cf2 - cs2));
+  flag = ((bt2 > eps * b2) || (fabs(gamma * pr - bx2) > eps * gamma * pr));
+  const double alphaf = flag ? (sqrt(fabs(a2 - cs2)) * denom) : 1.0;
+  const double alphas = flag ? (sqrt(fabs(cf2 - a2)) * denom) : 0.0;
+  const double sgnbx = (bx > 0) ? (1.0) : (-1.0);
+  const double cfalf = cf * alphaf;
+  const double csals = cs * alphas;
+  const double aaalf = aa * alphaf;
+  const double aaals = aa * alphas;
+  denom = 0.5 / a2;
+  // left eigenvectors (rows; k = 0..6 are mhd_eigen_st's l1..l7), non-zero entries
+  const double l0v = -cfalf * denom, l0t = +csals * denom * sgnbx * betay, l0u = +csals * denom * sgnbx * betaz;
+  const double l0b = +aaals * denom * isro * betay, l0c = +aaals * denom * isro * betaz, l0p = alphaf * denom * iro;
+  const double l1t = -0.5 * betaz, l1u = +0.5 * betay;
+  const double l1b = -0.5 * isro * betaz * sgnbx, l1c = +0.5 * isro * betay * sgnbx;
+  const double l2v = -csals * denom, l2t = -cfalf * denom * sgnbx * betay, l2u = -cfalf * denom * sgnbx * betaz;
+  const double l2b = -aaalf * denom * isro * betay, l2c = -aaalf * denom * isro * betaz, l2p = alphas * denom * iro;
+  const double l3p = -1.0 / a2;
+  double wl[7], wr[7];
+  bool zvn = true, zvt = true, zvu = true, zbt = true, zbu = true;
+  {  // the six waves that see (vn, vt, vu, bt, bu, pr): l1..l3, l5..l7 (mirror signs)
+    double w0[5], w6[5], w2[5], w4[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const double n_ = P(1, m), t_ = P(2, m), u_ = P(3, m), b_ = P(4, m), c_ = P(5, m), p_ = P(6, m);
+      zvn = zvn && (n_ == 0.0);
+      zvt = zvt && is_zero(t_);
+      zvu = zvu && is_zero(u_);
+      zbt = zbt && (b_ == 0.0);
+      zbu = zbu && (c_ == 0.0);
+      w0[m] = ((((l0v * n_ + l0t * t_) + l0u * u_) + l0b * b_) + l0c * c_) + l0p * p_;
+      w6[m] = (((((-l0v) * n_ + (-l0t) * t_) + (-l0u) * u_) + l0b * b_) + l0c * c_) + l0p * p_;
+      w2[m] = ((((l2v * n_ + l2t * t_) + l2u * u_) + l2b * b_) + l2c * c_) + l2p * p_;
+      w4[m] = (((((-l2v) * n_ + (-l2t) * t_) + (-l2u) * u_) + l2b * b_) + l2c * c_) + l2p * p_;
+    }
+    nl_lr<ODR>(w0, wl[0], wr[0]);
+    nl_lr<ODR>(w6, wl[6], wr[6]);
+    nl_lr<ODR>(w2, wl[2], wr[2]);
+    nl_lr<ODR>(w4, wl[4], wr[4]);
+  }
+  {  // the Alfven waves l2, l6 (vt, vu, bt, bu) and the entropy wave l4 (ro, pr)
+    double w1[5], w5[5], w3[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      const double t_ = P(2, m), u_ = P(3, m), b_ = P(4, m), c_ = P(5, m);
+      w1[m] = ((l1t * t_ + l1u * u_) + l1b * b_) + l1c * c_;
+      w5[m] = (((-l1t) * t_ + (-l1u) * u_) + l1b * b_) + l1c * c_;
+      w3[m] = P(0, m) + l3p * P(6, m);
+    }
+    nl_lr<ODR>(w1, wl[1], wr[1]);
+    nl_lr<ODR>(w5, wl[5], wr[5]);
+    nl_lr<ODR>(w3, wl[3], wr[3]);
+  }
+  // right eigenvectors (columns; r1..r7 of mhd_eigen_st), non-zero entries
+  const double r0r = ro * alphaf, r0v = -cfalf, r0t = +csals * sgnbx * betay, r0u = +csals * sgnbx * betaz;
+  const double r0b = +aaals * sro * betay, r0c = +aaals * sro * betaz, r0p = alphaf * gamma * pr;
+  const double r1t = -betaz, r1u = +betay, r1b = -sro * betaz * sgnbx, r1c = +sro * betay * sgnbx;
+  const double r2r = ro * alphas, r2v = -csals, r2t = -cfalf * sgnbx * betay, r2u = -cfalf * sgnbx * betaz;
+  const double r2b = -aaalf * sro * betay, r2c = -aaalf * sro * betaz, r2p = alphas * gamma * pr;
+  auto back = [&](const double w[7], double u[7]) {
+    u[0] = (((r0r * w[0] + r2r * w[2]) + w[3]) + r2r * w[4]) + r0r * w[6];
+    u[1] = ((r0v * w[0] + r2v * w[2]) + (-r2v) * w[4]) + (-r0v) * w[6];
+    u[2] = (((((r0t * w[0] + r1t * w[1]) + r2t * w[2]) + (-r2t) * w[4]) + (-r1t) * w[5]) + (-r0t) * w[6]);
+    u[3] = (((((r0u * w[0] + r1u * w[1]) + r2u * w[2]) + (-r2u) * w[4]) + (-r1u) * w[5]) + (-r0u) * w[6]);
+    u[4] = (((((r0b * w[0] + r1b * w[1]) + r2b * w[2]) + r2b * w[4]) + r1b * w[5]) + r0b * w[6]);
+    u[5] = (((((r0c * w[0] + r1c * w[1]) + r2c * w[2]) + r2c * w[4]) + r1c * w[5]) + r0c * w[6]);
+    u[6] = ((r0p * w[0] + r2p * w[2]) + r2p * w[4]) + r0p * w[6];
+  };
+  back(wl, vl);
+  back(wr, vr);
+  if (zvn) { vl[1] = 0.0; vr[1] = 0.0; }
+  if (zvt) { vl[2] = 0.0; vr[2] = 0.0; }
+  if (zvu) { vl[3] = 0.0; vr[3] = 0.0; }
+  if (zbt) { vl[4] = 0.0; vr[4] = 0.0; }
+  if (zbu) { vl[5] = 0.0; vr[5] = 0.0; }
+  const double peps = 1e-12;
+  if (vl[0] <= peps || vl[6] <= peps) {
+    vl[0] = ro;
+    vl[1] = vn;
+    vl[6] = pr;
+  }
+  if (vr[0] <= peps || vr[6] <= peps) {
     vr[0] = ro;
     vr[1] = vn;
     vr[6] = pr;

@@ -100,7 +100,8 @@ struct View {
   // per-cell viscosity / resistivity of the dissipative drivers (the API's nu/eta), or null
   // for the uniform nu0/eta0 of the run options
   const double *nu, *eta;
-  int recon;  // face-value reconstruction: 0 characteristic (mhd_m/a_reconst), 1 primitive (mhd_reconst)
+  int recon;  // face-value reconstruction: 0 characteristic (mhd_m/a_reconst), 1 primitive (mhd_reconst),
+              // 2 Athena-type characteristic (mhd_c_reconst)
 };
 
 __device__ __forceinline__ long long cidx(const Geo &g, int i, int j, int k)
@@ -311,15 +312,18 @@ struct LrStencil {
   __device__ __forceinline__ double late(int f, int m) const { return field(f)[c + (m - 2) * s]; }
 };
 
-// PR: the face-value form, 0 characteristic, 1 primitive, -1 chosen at run time by v.recon (the
-// forms whose instances may differ per launch); the default kernels take it as a template
-// argument so the characteristic code is compiled without the other branch
+// PR: the face-value form, 0 characteristic (mhd_m/a_reconst), 1 primitive (mhd_reconst), 2
+// Athena-type characteristic (mhd_c_reconst), -1 chosen at run time by v.recon (the forms whose
+// instances may differ per launch); the default kernels take it as a template argument so the
+// characteristic code is compiled without the other branches
 template <int ODR, int A, int PR = -1, class ST>
 __device__ __forceinline__ void lr_cell(const View &v, long long c, long long s, const ST &st, double cnc)
 {
   double vl[7], vr[7];
-  if (PR == 1 || (PR < 0 && v.recon))
+  if (PR == 1 || (PR < 0 && v.recon == 1))
     face_states_prim<ODR>(st, vl, vr);
+  else if (PR == 2 || (PR < 0 && v.recon == 2))
+    face_states_athena<ODR>(st, cnc, v.gam, vl, vr);
   else
     face_states_grouped<ODR>(st, cnc, v.gam, vl, vr);
 #pragma unroll
@@ -519,8 +523,10 @@ __device__ __forceinline__ void cell_states(const View &v, long long c, double v
   const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
   const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
   const LrStencil<A> st{v, c, s};
-  if (v.recon)
+  if (v.recon == 1)
     face_states_prim<ODR>(st, vl, vr);
+  else if (v.recon == 2)
+    face_states_athena<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
   else
     face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
   if (g.dim >= 2) {

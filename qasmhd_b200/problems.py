@@ -42,7 +42,9 @@ class Problem:
     odr: int = 4
     rk: int = 3
     ctw: int = 1
-    char_mode: int = 0  # face values in characteristic (0) or primitive (1) variables
+    # face values: characteristic (0, mhd_m/a_reconst), primitive (1, mhd_reconst) or Athena-type
+    # characteristic (2, mhd_c_reconst) variables
+    char_mode: int = 0
     gam: float = 5.0 / 3.0
     cfl: float = 0.4
     dtrec: float = 1.0

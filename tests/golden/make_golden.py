@@ -8,6 +8,7 @@ and numpy seeds; the fixtures store the outputs plus a SHA-256 of each input
 so a drift of the generators is caught.
 
 Run from the repository root:  python tests/golden/make_golden.py
+(``--kat <name>`` or ``--steps <case> ...`` regenerate only those fixtures).
 """
 from __future__ import annotations
 
@@ -54,7 +55,7 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
         a = rng.normal(0, 1, (n, 5))
         a[::7] = a[::7, :1]       # constant stencils
         return a
-    if kind in ("lrstate", "lrstate_prim"):
+    if kind in ("lrstate", "lrstate_prim", "lrstate_char"):
         ro = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.1
         rest = rng.normal(0, 1, (n, 25))
         pr = np.abs(rng.normal(1, 0.3, (n, 5))) + 0.05
@@ -79,7 +80,8 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
 
 
 KAT_FUNCS = {"flux": ([0, 1, 2, 3], 7), "interp": (list(range(10, 20)), 2), "lrstate": ([20, 21, 22, 23], 14),
-             "lrstate_prim": ([24, 25, 26, 27], 14), "cuct": ([30], 1), "energy": ([31, 32], 1)}
+             "lrstate_prim": ([24, 25, 26, 27], 14), "lrstate_char": ([40, 41, 42, 43], 14), "cuct": ([30], 1),
+             "energy": ([31, 32], 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -106,6 +108,12 @@ def _prim(p):
     return p
 
 
+def _char(p):
+    """The Athena-type characteristic reconstruction (mhd_c_reconst)."""
+    p.char_mode = 2
+    return p
+
+
 def _wave_bc(dim, seed):
     rng = np.random.default_rng(seed)
 
@@ -127,6 +135,10 @@ STEP_CASES = [
     ("bw1d_prim", lambda: _prim(P.brio_wu(64)), R.MODE_RUN, 5),
     ("ot2d_prim", lambda: _prim(P.orszag_tang(16)), R.MODE_RUN, 3),
     ("kh3d_prim", lambda: _prim(P.kelvin_helmholtz(3, 6, mach=0.3, rmn=P.RMN_MLAU)), R.MODE_RUN, 2),
+    ("bw1d_char", lambda: _char(P.brio_wu(64)), R.MODE_RUN, 5),
+    ("ot2d_char", lambda: _char(P.orszag_tang(16)), R.MODE_RUN, 3),
+    ("kh2d_char_roe", lambda: _char(P.kelvin_helmholtz(2, 16, mach=0.3, rmn=P.RMN_ROE)), R.MODE_RUN, 3),
+    ("kh3d_char", lambda: _char(P.kelvin_helmholtz(3, 6, mach=0.3, rmn=P.RMN_MLAU)), R.MODE_RUN, 2),
     ("hall1d_exec", lambda: P.hall_shock(64, di=1e-3, tmax=0.02), R.MODE_EXEC, 0),
     ("hall1d_de_run", lambda: P.hall_shock(64, di=0.01, d_ele=2.0), R.MODE_RUN, 4),
     *[(f"ot2d_rmn{r}", (lambda r=r: P.orszag_tang(16, rmn=r)), R.MODE_RUN, 3) for r in range(4)],
@@ -158,8 +170,20 @@ def make_kat_prim() -> None:
     print("kat lrstate_prim", inp.shape)
 
 
+def make_kat_char() -> None:
+    """mhd_lrstate with the Athena-type reconstruction: the harness's ids 20..23 built against
+    mhd_c_reconst (oracle/_ref/ref_kat_char), stored as 40..43 (the oracle's ids for that form)."""
+    inp = kat_inputs("lrstate_char")
+    exe = os.path.join(R.REF_DIR, "ref_kat_char")
+    outs = {f"f{f + 20}": R.run_kat(f, inp, 14, exe=exe) for f in (20, 21, 22, 23)}
+    np.savez_compressed(os.path.join(OUT, "kat_lrstate_char.npz"), input_sha=sha(inp), **outs)
+    print("kat lrstate_char", inp.shape)
+
+
 def make_kat(name: str) -> None:
     """One point-function fixture, kat_<name>.npz."""
+    if name in ("lrstate_prim", "lrstate_char"):
+        return make_kat_prim() if name == "lrstate_prim" else make_kat_char()
     funcs, nout = KAT_FUNCS[name]
     inp = kat_inputs(name)
     outs = {f"f{f}": R.run_kat(f, inp, nout) for f in funcs}
@@ -167,18 +191,39 @@ def make_kat(name: str) -> None:
     print("kat", name, inp.shape)
 
 
+def add_steps(names) -> None:
+    """Recompute the named step cases only, keeping the others of steps.npz."""
+    path = os.path.join(OUT, "steps.npz")
+    data = dict(np.load(path)) if os.path.exists(path) else {}
+    for name, build, mode, nsteps in STEP_CASES:
+        if name not in names:
+            continue
+        p = build()
+        r = R.run_reference(p, mode, nsteps=nsteps, nthreads=4)
+        data[f"{name}__state"] = r["state"]
+        data[f"{name}__dts"] = r["dts"]
+        data[f"{name}__meta"] = np.array([r["steps"], r["tim"], r["dt"]])
+        data[f"{name}__insha"] = np.array(sha(p.state))
+        print("step", name, p.nd, r["steps"])
+    np.savez_compressed(path, **data)
+
+
 def main() -> None:
     if len(sys.argv) > 2 and sys.argv[1] == "--kat":  # one fixture only
         make_kat(sys.argv[2])
         return
+    if len(sys.argv) > 2 and sys.argv[1] == "--steps":  # some step cases only
+        add_steps(sys.argv[2:])
+        return
     for name, (funcs, nout) in KAT_FUNCS.items():
-        if name == "lrstate_prim":
+        if name in ("lrstate_prim", "lrstate_char"):
             continue
         inp = kat_inputs(name)
         outs = {f"f{f}": R.run_kat(f, inp, nout) for f in funcs}
         np.savez_compressed(os.path.join(OUT, f"kat_{name}.npz"), input_sha=sha(inp), **outs)
         print("kat", name, inp.shape)
     make_kat_prim()
+    make_kat_char()
     data = {}
     for name, build, mode, nsteps in STEP_CASES:
         p = build()

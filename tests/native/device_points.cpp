@@ -1,7 +1,7 @@
 // Host build of the device point functions of the step (qas_device.cuh is host+device): the
 // Riemann solvers, the face interpolations, the characteristic face states (both the
-// per-field and the grouped-stencil forms the kernels use), the primitive-variable face states
-// and the CUCT weight, with the
+// per-field and the grouped-stencil forms the kernels use), the primitive-variable and the
+// Athena-type characteristic face states and the CUCT weight, with the
 // argument layout of the known-answer vectors of the reference's own point functions.
 #include "qas_device.cuh"
 
@@ -70,6 +70,18 @@ void t_face_states(int odr, int grouped, const double *a, double *o)
     case 2: face_states_of<2>(a, grouped, o); break;
     case 3: face_states_of<3>(a, grouped, o); break;
     default: face_states_of<4>(a, grouped, o); break;
+  }
+}
+
+// the same with the Athena-type characteristic reconstruction (mhd_c_reconst, mhd_eigen_st)
+void t_face_states_char(int odr, const double *a, double *o)
+{
+  const ArrayStencil st{a};
+  switch (odr) {
+    case 1: face_states_athena<1>(st, a[35], a[36], &o[0], &o[7]); break;
+    case 2: face_states_athena<2>(st, a[35], a[36], &o[0], &o[7]); break;
+    case 3: face_states_athena<3>(st, a[35], a[36], &o[0], &o[7]); break;
+    default: face_states_athena<4>(st, a[35], a[36], &o[0], &o[7]); break;
   }
 }
 

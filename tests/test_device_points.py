@@ -7,7 +7,8 @@ square root) is compared with the known-answer vectors of the reference's point 
 built from source): the four Riemann solvers, the linear and nonlinear face interpolations the
 schemes use, the characteristic face states of mhd_lrstate at every order -- the per-field
 form and the grouped-stencil form the kernels run --, the primitive-variable face states of
-its mhd_reconst form (qas_scheme.char_mode = 1) and the CUCT weight."""
+its mhd_reconst form (qas_scheme.char_mode = 1), its mhd_c_reconst form (char_mode = 2) and the
+CUCT weight."""
 import ctypes
 import os
 import shutil
@@ -40,6 +41,7 @@ def dev(tmp_path_factory):
         f.argtypes = [ctypes.c_int, D, D]
     lib.t_face_states.argtypes = [ctypes.c_int, ctypes.c_int, D, D]
     lib.t_face_states_prim.argtypes = [ctypes.c_int, D, D]
+    lib.t_face_states_char.argtypes = [ctypes.c_int, D, D]
     return lib
 
 
@@ -82,6 +84,15 @@ def test_primitive_face_states(dev, odr):
     inp = G.kat_inputs("lrstate_prim")
     gold = np.load(os.path.join(GOLD, "kat_lrstate_prim.npz"))[f"f{23 + odr}"]
     assert_bitwise(_run(dev.t_face_states_prim, inp, 14, odr), gold, f"primitive face states order {odr}")
+
+
+@pytest.mark.parametrize("odr", [1, 2, 3, 4])
+def test_athena_face_states(dev, odr):
+    """mhd_lrstate with mhd_c_reconst (the reference's known answers from the harness built against
+    it), the device face_states_athena of qas_scheme.char_mode = 2."""
+    inp = G.kat_inputs("lrstate_char")
+    gold = np.load(os.path.join(GOLD, "kat_lrstate_char.npz"))[f"f{39 + odr}"]
+    assert_bitwise(_run(dev.t_face_states_char, inp, 14, odr), gold, f"Athena-type face states order {odr}")
 
 
 def test_cuct_weight(dev):

@@ -130,14 +130,16 @@ def test_live_reference_dissipation_profiles(restatement, dim):
 
 @pytest.mark.skipif(not R.reference_available(2, 1, gravity="prim"), reason="reference prim builds not built")
 @pytest.mark.parametrize("dim", [1, 2, 3])
-def test_live_reference_primitive_reconstruction(restatement, dim):
-    """mhd_lrstate with mhd_reconst (primitive variables) in place of mhd_m/a_reconst."""
+@pytest.mark.parametrize("mode", [1, 2])
+def test_live_reference_other_reconstructions(restatement, dim, mode):
+    """mhd_lrstate with mhd_reconst (mode 1, primitive variables) or mhd_c_reconst (mode 2,
+    Athena-type eigenvectors) in place of mhd_m/a_reconst, against the reference built so."""
     p = {1: lambda: P.brio_wu(64), 2: lambda: P.orszag_tang(20, rmn=P.RMN_ROE),
          3: lambda: P.kelvin_helmholtz(3, 8, mach=0.3, rmn=P.RMN_LHLLD)}[dim]()
-    p.char_mode = 1
+    p.char_mode = mode
     a = R.run_reference(p, R.MODE_RUN, nsteps=3, nthreads=2)
     b = restatement.run(p, 3, mode=R.MODE_RUN)
-    assert_bitwise(b["state"], a["state"], f"prim {dim}d")
+    assert_bitwise(b["state"], a["state"], f"char_mode {mode} {dim}d")
 
 
 @pytest.mark.skipif(R.o3_binary(2) is None or R.o3_binary(3) is None, reason="no -O3 timing build for this host")

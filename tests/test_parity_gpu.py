@@ -401,12 +401,14 @@ def test_primitives_readback(grav):
 
 
 @pytest.mark.parametrize("case", ["bw1d", "ot2d", "kh3d_mlau", "ot2d_fused", "ot2d_staged"])
-def test_primitive_reconstruction(restatement, case):
-    """char_mode = 1: face values by mhd_reconst (each primitive on its own), every form."""
+@pytest.mark.parametrize("mode", [1, 2])
+def test_other_reconstructions(restatement, case, mode):
+    """char_mode = 1: face values by mhd_reconst (each primitive on its own); char_mode = 2: by
+    mhd_c_reconst (Athena-type eigenvectors for every state); every form."""
     p = {"bw1d": lambda: P.brio_wu(128), "ot2d": lambda: P.orszag_tang(64, rmn=P.RMN_HLLD),
          "kh3d_mlau": lambda: P.kelvin_helmholtz(3, 16, mach=0.3), "ot2d_fused": lambda: P.orszag_tang(64),
          "ot2d_staged": lambda: P.orszag_tang(64)}[case]()
-    p.char_mode = 1
+    p.char_mode = mode
     a = restatement.run(p, 4, mode=R.MODE_RUN)
     with L.Context.from_problem(p) as ctx:
         if case.endswith("fused"):
@@ -416,4 +418,4 @@ def test_primitive_reconstruction(restatement, case):
         ctx.upload(p.state)
         ctx.run(max_steps=4, flg=p.flg, stop_rule=0, cfl=p.cfl, use_graph=not case.endswith("fused"))
         b = ctx.download(p.state.shape)
-    assert_bitwise(b, a["state"], f"prim {case}")
+    assert_bitwise(b, a["state"], f"char_mode {mode} {case}")
