@@ -38,26 +38,28 @@ ALG_BYTES_PER_CELL_UPDATE = 512  # 8 FP64 fields: stage 1 reads u^n, writes; sta
 #   k_flux   reads the 7+7 face states, the face normal field, the induction states (2/4), vn
 #            and the shock detector (MLAU/LHLLD: 1 in 2D, 2 in 3D); writes 8 fluxes and the
 #            central induction fluxes (1 in 2D, 2 in 3D)
-#   k_sweep  (face states + flux of one axis in one kernel) reads the 7 stencil fields, the
-#            centre and face normal fields, the shock detector; writes the fluxes and central
-#            induction fluxes: the face states never leave the SM
+#   k_sweep  (face states + flux of one axis in one kernel, the 3D default) reads the 7 stencil
+#            fields, the centre and face normal fields and the shock detector (1 in 2D, 2 in 3D,
+#            MLAU/LHLLD); writes 7 fluxes and the central induction fluxes (1 in 2D, 2 in 3D):
+#            the face states never leave the SM
 KERNEL_ARRAYS = {
     "k_lr": {1: 8 + 14, 2: 9 + 16, 3: 9 + 18},
     "k_flux": {1: 15 + 8, 2: 14 + 1 + 2 + 2 + 8 + 1, 3: 14 + 1 + 4 + 3 + 8 + 2},
-    "k_sweep": {1: 8 + 8, 2: 9 + 1 + 8 + 1, 3: 9 + 2 + 8 + 2},
+    "k_sweep": {1: 8 + 7, 2: 9 + 1 + 7 + 1, 3: 9 + 2 + 7 + 2},
 }
-# FP64 work of k_lr per cell, counted by ncu on the 2D Orszag-Tang 1024^2 workload
-# (ODR=4; profiles/k_lr_ot2d_1024.md): dadd + dmul + dfma instructions and flops
-# (a dfma counts 2).
-K_LR_FP64_INSTR_PER_CELL = 1054.0
-K_LR_FP64_FLOPS_PER_CELL = 1262.0
+# FP64 work per cell, counted by ncu (dadd + dmul + dfma instructions, and flops with a dfma
+# counted 2): k_lr on the 2D Orszag-Tang 1024^2 workload (ODR=4; profiles/k_lr_ot2d_1024.md),
+# k_sweep (MLAU) on KH 128^3 (profiles/k_sweep_kh3d_256.md: 1588-1604 per direction)
+FP64_INSTR_PER_CELL = {"k_lr": 1054.0, "k_sweep": 1600.0}
+FP64_FLOPS_PER_CELL = {"k_lr": 1262.0, "k_sweep": 1923.0}
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant kernel, per
-# workload: k_lr (y faces) of OT 1024^2 (profiles/k_lr_ot2d_1024.md) and of KH 3D: the KH 128^3
-# capture (x faces, 136^3 padded cells: 200.12 + 314.29 MB) scaled by padded cells to 264^3
-# (traffic per cell is size-independent: every array is streamed once, the 126 MB L2 holds no
-# full array)
+# workload: k_lr (y faces) of OT 1024^2 (profiles/k_lr_ot2d_1024.md); for KH 3D the KH 128^3
+# captures (136^3 padded cells: k_lr x faces 200.12 + 314.29 MB; k_sweep the mean of its x, y, z
+# launches, 378.0 + 405.8 + 405.0 MB / 3) scaled by padded cells to 264^3 (traffic per cell is
+# size-independent: every array is streamed once, the 126 MB L2 holds no full array)
 KERNEL_TRAFFIC_PER_LAUNCH = {("k_lr", "ot2d_1024"): 76.70e6 + 92.25e6,
-                             ("k_lr", "kh3d_256"): (200.12e6 + 314.29e6) * (264 / 136) ** 3}
+                             ("k_lr", "kh3d_256"): (200.12e6 + 314.29e6) * (264 / 136) ** 3,
+                             ("k_sweep", "kh3d_256"): (378.0e6 + 405.8e6 + 405.0e6) / 3 * (264 / 136) ** 3}
 
 
 def parse():
@@ -649,14 +651,13 @@ def main():
         "gpu_launches_basis": "kernel launches of one timed window of K steps",
         "clocks": clk,
     }
-    if "k_lr" in prof:
+    if dom in FP64_INSTR_PER_CELL:
+        # the dominant kernel is FP64-bound: its FP64 rate against the measured DFMA peak
         fp64_peak = L.fp64_peak_tflops()
-        lr_launches, lr_ms = prof["k_lr"]
-        lr_ms_launch = lr_ms / lr_launches
-        lr_tflops = K_LR_FP64_FLOPS_PER_CELL * prob.nd / (lr_ms_launch * 1e-3) / 1e12
-        lr_pipe = K_LR_FP64_INSTR_PER_CELL * prob.nd / (lr_ms_launch * 1e-3) / (fp64_peak * 1e12 / 2.0)
-        line["fp64"] = {"kernel": "k_lr", "achieved_tflops": lr_tflops, "peak_tflops": fp64_peak,
-                        "frac": lr_tflops / fp64_peak, "pipe_frac": lr_pipe,
+        tflops = FP64_FLOPS_PER_CELL[dom] * prob.nd / (dom_ms_launch * 1e-3) / 1e12
+        pipe = FP64_INSTR_PER_CELL[dom] * prob.nd / (dom_ms_launch * 1e-3) / (fp64_peak * 1e12 / 2.0)
+        line["fp64"] = {"kernel": dom, "achieved_tflops": tflops, "peak_tflops": fp64_peak,
+                        "frac": tflops / fp64_peak, "pipe_frac": pipe,
                         "basis": "ncu-counted FP64 flops per cell x cells / live launch time; peak = measured DFMA "
                                  "throughput (qas_fp64_peak); pipe_frac = FP64 instructions vs the DFMA issue rate"}
     if rank == 0 and not args.no_cpu_baseline and world == 1:

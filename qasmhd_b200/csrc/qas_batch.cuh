@@ -39,6 +39,28 @@ __device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, 
   }
 }
 
+// Block loop of a persistent batched kernel.  QAS_BATCH_CONTIGUOUS = 1: each CTA takes one
+// contiguous run of the (instance-major) block list, so its consecutive blocks share an
+// instance and that instance's View, control word and launch grid stay in L1; the next map
+// entry is loaded while the current block works.  0: grid-stride over the list.
+#ifndef QAS_BATCH_CONTIGUOUS
+#define QAS_BATCH_CONTIGUOUS 1
+#endif
+#if QAS_BATCH_CONTIGUOUS
+#define QAS_BATCH_BLOCKS(map)                                                         \
+  const int bper_ = ((map).nblocks + gridDim.x - 1) / gridDim.x;                      \
+  const int bend_ = min((map).nblocks, (int)(blockIdx.x + 1) * bper_);                \
+  int2 bnext_ = make_int2(0, 0);                                                      \
+  if ((int)blockIdx.x * bper_ < bend_) bnext_ = (map).blk[blockIdx.x * bper_];       \
+  for (int b_ = blockIdx.x * bper_; b_ < bend_; b_++) {                               \
+    const int2 bi_ = bnext_;                                                          \
+    if (b_ + 1 < bend_) bnext_ = (map).blk[b_ + 1];                                   \
+    const View &v = views[bi_.x];                                                     \
+    if (v.ctl->done) continue;                                                        \
+    const int4 gd_ = (map).grid[bi_.x];                                               \
+    int ti, tj, tk;                                                                   \
+    batch_thread(gd_, bi_.y, ti, tj, tk);
+#else
 #define QAS_BATCH_BLOCKS(map)                                                         \
   for (int b_ = blockIdx.x; b_ < (map).nblocks; b_ += gridDim.x) {                    \
     const int2 bi_ = (map).blk[b_];                                                   \
@@ -47,6 +69,7 @@ __device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, 
     const int4 gd_ = (map).grid[bi_.x];                                               \
     int ti, tj, tk;                                                                   \
     batch_thread(gd_, bi_.y, ti, tj, tk);
+#endif
 
 #define QAS_BATCH_END }
 
