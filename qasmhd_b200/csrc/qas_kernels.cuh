@@ -578,6 +578,24 @@ __device__ __forceinline__ void face_flux(const View &v, long long f, const doub
   riemann_out<RMN>(L, R, bn, v.gam, dv0, dv1, FaceSink<A, false>{v, f, s, QL[0], QR[0], QL[1], QR[1], 0.0});
 }
 
+// one lane of an x-sweep warp: the face states of cell (i, j, k) (a valid cell even for a lane
+// past the end, have_cell false, so that the warp stays converged), the hand-off of the right-face
+// state to the next lane, and the flux at the cell's left face when the previous lane holds the
+// cell to its left (i >= 3)
+template <int ODR, int RMN>
+__device__ __forceinline__ void sweep_x_cell(const View &v, int i, int j, int k, int lane, bool have_cell)
+{
+  const long long c = cidx(v.g, i, j, k);
+  double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+  cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
+  double L[7], QL[2];
+#pragma unroll
+  for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
+  QL[0] = __shfl_up_sync(0xffffffffu, ql[0], 1);
+  QL[1] = __shfl_up_sync(0xffffffffu, ql[1], 1);
+  if (lane >= 1 && have_cell && i >= 3) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
+}
+
 // x sweep: 4 warps per block, 31 faces per warp over the flattened cells of all rows
 template <int ODR, int RMN>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_x(View v, long long nwarps)
@@ -594,33 +612,16 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_x(View v,
   if (!have_cell) t = total - 1;  // a valid cell, computed and discarded (keeps the warp converged)
   const long long row = t / ncell;
   const int i = 2 + (int)(t - row * ncell);
-  const long long c = cidx(g, i, (int)(row % g.ny), (int)(row / g.ny));
-  double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
-  cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
-  double L[7], QL[2];
-#pragma unroll
-  for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
-  QL[0] = __shfl_up_sync(0xffffffffu, ql[0], 1);
-  QL[1] = __shfl_up_sync(0xffffffffu, ql[1], 1);
-  // lane-1 holds cell i-1 of the same row exactly when i >= 3
-  if (lane >= 1 && have_cell && i >= 3) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
+  sweep_x_cell<ODR, RMN>(v, i, (int)(row % g.ny), (int)(row / g.ny), lane, have_cell);
 }
 
-// y / z sweep: one thread per column, marching over `seg` faces along A
+// one column of a y / z sweep: the faces p in [p0, p1) along A of the column through (i, o)
+// (o = k for the y sweep, j for the z sweep), from the cell before p0 on; the previous cell's
+// right-face state waits in the thread's shared-memory slot carry[.][tid]
 template <int ODR, int RMN, int A>
-__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v, int seg)
+__device__ __forceinline__ void sweep_column(const View &v, int i, int o, int p0, int p1, double (*carry)[128], int tid)
 {
-  if (v.ctl->done) return;
   const Geo &g = v.g;
-  __shared__ double carry[9][128];  // previous cell's right-face state and induction state, per thread
-  const int tid = threadIdx.x;
-  const int no = A == 1 ? g.nz : g.ny;  // extent of the other transverse axis
-  const long long col = (long long)blockIdx.x * 128 + tid;
-  if (col >= (long long)g.nx * no) return;  // no barrier below: threads leave freely
-  const int i = (int)(col % g.nx), o = (int)(col / g.nx);
-  const int n = g.n[A];
-  const int p0 = 3 + blockIdx.y * seg;
-  const int p1 = min(p0 + seg, n - 2);
   const long long s = g.s[A];
   long long c = A == 1 ? cidx(g, i, p0 - 1, o) : cidx(g, i, o, p0 - 1);
   {
@@ -647,6 +648,21 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v,
     carry[8][tid] = ql[1];
     face_flux<RMN, A>(v, c, L, vr, QL, qr);
   }
+}
+
+// y / z sweep: one thread per column, marching over `seg` faces along A
+template <int ODR, int RMN, int A>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v, int seg)
+{
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  __shared__ double carry[9][128];  // previous cell's right-face state and induction state, per thread
+  const int tid = threadIdx.x;
+  const int no = A == 1 ? g.nz : g.ny;  // extent of the other transverse axis
+  const long long col = (long long)blockIdx.x * 128 + tid;
+  if (col >= (long long)g.nx * no) return;  // no barrier below: threads leave freely
+  const int p0 = 3 + blockIdx.y * seg;
+  sweep_column<ODR, RMN, A>(v, (int)(col % g.nx), (int)(col / g.nx), p0, min(p0 + seg, g.n[A] - 2), carry, tid);
 }
 
 // ---------------------------------------------------------------------------

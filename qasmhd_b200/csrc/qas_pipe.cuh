@@ -109,6 +109,69 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, 
   flux_body<3, A>(v, i, j, k);
 }
 
+// fused face sweeps on a window (the default form in 3D, see k_sweep_x / k_sweep_m)
+// x sweep over the flattened cells of the rows of planes r
+template <int ODR, int RMN>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_x(View v, Rows2 r, long long nwarps)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  const int lane = threadIdx.x & 31;
+  const long long w = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (w >= nwarps) return;  // the whole warp leaves together
+  const long long ncell = g.nx - 4;
+  const long long per_plane = g.dim == 3 ? g.ny : 1;
+  const long long total = ncell * per_plane * (rows_len(r.a) + rows_len(r.b));
+  long long t = w * 31 + lane;
+  const bool have_cell = t < total;
+  if (!have_cell) t = total - 1;
+  const long long row = t / ncell;
+  const int i = 2 + (int)(t - row * ncell);
+  const int j = g.dim == 3 ? (int)(row % g.ny) : rows2_plane(r, (int)row);
+  const int k = g.dim == 3 ? rows2_plane(r, (int)(row / g.ny)) : 0;
+  sweep_x_cell<ODR, RMN>(v, i, j, k, lane, have_cell);
+}
+
+// y sweep of a 3D window (an in-plane axis): columns (i, k) with k on planes r, every y face
+// [3, ny-2) in segments of `seg`
+template <int ODR, int RMN>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_y3(View v, Rows2 r, int seg)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  __shared__ double carry[9][128];
+  const int tid = threadIdx.x;
+  const long long col = (long long)blockIdx.x * 128 + tid;
+  if (col >= (long long)g.nx * (rows_len(r.a) + rows_len(r.b))) return;
+  const int p0 = 3 + blockIdx.y * seg;
+  sweep_column<ODR, RMN, 1>(v, (int)(col % g.nx), rows2_plane(r, (int)(col / g.nx)), p0, min(p0 + seg, g.ny - 2),
+                            carry, tid);
+}
+
+// sweep along the last axis A (y in 2D, z in 3D): every column (i, j in 3D), the faces of
+// f = r clipped to [3, n-2), chunk q of `seg` faces per blockIdx.y: first those of r.a, then r.b
+template <int ODR, int RMN, int A>
+__global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_last(View v, Rows2 f, int seg)
+{
+  QAS_PDL_WAIT();
+  if (v.ctl->done) return;
+  const Geo &g = v.g;
+  __shared__ double carry[9][128];
+  const int tid = threadIdx.x;
+  const long long col = (long long)blockIdx.x * 128 + tid;
+  if (col >= (long long)g.nx * (A == 2 ? g.ny : 1)) return;
+  const int n = g.n[A];
+  const Rows a{max(f.a.lo, 3), min(f.a.hi, n - 2)}, b{max(f.b.lo, 3), min(f.b.hi, n - 2)};
+  const int ca = (rows_len(a) + seg - 1) / seg;
+  const int q = blockIdx.y;
+  const Rows &x = q < ca ? a : b;
+  const int p0 = x.lo + (q < ca ? q : q - ca) * seg;
+  if (p0 >= x.hi) return;
+  sweep_column<ODR, RMN, A>(v, (int)(col % g.nx), (int)(col / g.nx), p0, min(p0 + seg, x.hi), carry, tid);
+}
+
 template <int ODR>
 __global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows2 r)
 {

@@ -62,11 +62,13 @@ def _block(p, pinned):
     return t.numpy(), t  # keep the tensor alive beside its view
 
 
-def _piped(p, nsteps, items=None, alias=True, pinned=False, replan_at=None, lanes=None):
+def _piped(p, nsteps, items=None, alias=True, pinned=False, replan_at=None, lanes=None, fused=None):
     h, keep_h = _block(p, pinned)
     out, keep_o = (h, None) if alias else _block(p, pinned)
     states, infos = [], []
     with L.Context.from_problem(p) as ctx:
+        if fused is not None:
+            ctx.set_option(L.QAS_OPT_FUSED_SWEEP, fused)
         if lanes is not None:
             ctx.set_option(L.QAS_OPT_PIPE_LANES, lanes)
         if items is not None:
@@ -95,6 +97,19 @@ def _compare(a, b, label):
 def test_step_host_matches_serial_composition(case):
     p = CASES[case]()
     _compare(_serial(p, 5), _piped(p, 5), case)
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("case,fused", [("ot2d_96x160_roe_ctw0", 1), ("kh2d_64x128_mlau_open_y", 1),
+                                        ("kh3d_16x16x96_mlau", 0), ("wave3d_20_open_z_roe", 0)])
+def test_step_host_sweep_forms(case, fused, pinned):
+    """The wave's face sweeps in the form that is not the dimension's default (fused windows in
+    2D: x rows of the window's planes and the last-axis march over its faces; two kernels in 3D)
+    give the serial composition's bits as well."""
+    if pinned:
+        pytest.importorskip("torch")
+    p = CASES[case]()
+    _compare(_serial(p, 5), _piped(p, 5, items=12, pinned=pinned, fused=fused), f"{case} fused={fused}")
 
 
 @pytest.mark.parametrize("items", [1, 2, 3, 5, 16, 64])
