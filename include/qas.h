@@ -256,7 +256,8 @@ qas_status qas_set_gravity(qas_ctx *ctx, const double *phi_g);
 /* Tuning options (defaults are the measured best on B200).
  *   QAS_OPT_FUSED_SWEEP: 0 = reconstruction and Riemann flux of each direction in two
  *   kernels with the face states in HBM (default in 1D and 2D); 1 = one fused sweep kernel
- *   per direction, the face states kept on chip (default in 3D).
+ *   per direction, the face states kept on chip (default in 3D; 4th-order interpolation only,
+ *   other orders keep the two kernels).
  *   QAS_OPT_LR_STAGING: 1 = the reconstruction stages its stencils in shared memory with
  *   TMA tensor copies (available for 2D/3D, 4th-order interpolation, even padded x extent;
  *   QAS_ERR_UNSUPPORTED otherwise); 0 = it reads them from global memory (default: measured

@@ -515,44 +515,35 @@ int sweep_seg(qas_ctx *c, int a, const void *fn)
 #ifndef QAS_SWEEP_CARVEOUT
 #define QAS_SWEEP_CARVEOUT -1
 #endif
-// choose the y / z segment lengths outside any stream capture (occupancy query)
-template <int ODR, int RMN>
+// choose the y / z segment lengths outside any stream capture (occupancy query); the fused
+// sweeps are built for 4th-order interpolation only (other orders take the two-kernel form)
+template <int RMN>
 void sweep_prepare_t(qas_ctx *c)
 {
   if (QAS_SWEEP_CARVEOUT >= 0) {
-    cudaFuncSetAttribute((const void *)k_sweep_x<ODR, RMN>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         QAS_SWEEP_CARVEOUT);
-    cudaFuncSetAttribute((const void *)k_sweep_m<ODR, RMN, 1>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         QAS_SWEEP_CARVEOUT);
-    cudaFuncSetAttribute((const void *)k_sweep_m<ODR, RMN, 2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         QAS_SWEEP_CARVEOUT);
+    const void *fns[6] = {(const void *)k_sweep_x<4, RMN, 0>, (const void *)k_sweep_m<4, RMN, 1, 0>,
+                          (const void *)k_sweep_m<4, RMN, 2, 0>, (const void *)k_sweep_x<4, RMN, -1>,
+                          (const void *)k_sweep_m<4, RMN, 1, -1>, (const void *)k_sweep_m<4, RMN, 2, -1>};
+    for (const void *f : fns)
+      cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, QAS_SWEEP_CARVEOUT);
     cudaGetLastError();
   }
-  if (c->geo.dim >= 2) sweep_seg(c, 1, (const void *)k_sweep_m<ODR, RMN, 1>);
-  if (c->geo.dim >= 3) sweep_seg(c, 2, (const void *)k_sweep_m<ODR, RMN, 2>);
-}
-template <int ODR>
-void sweep_prepare_o(qas_ctx *c)
-{
-  switch (c->scheme.rmn) {
-    case 0: sweep_prepare_t<ODR, 0>(c); break;
-    case 1: sweep_prepare_t<ODR, 1>(c); break;
-    case 2: sweep_prepare_t<ODR, 2>(c); break;
-    default: sweep_prepare_t<ODR, 3>(c); break;
-  }
+  if (c->geo.dim >= 2) sweep_seg(c, 1, (const void *)k_sweep_m<4, RMN, 1, 0>);
+  if (c->geo.dim >= 3) sweep_seg(c, 2, (const void *)k_sweep_m<4, RMN, 2, 0>);
 }
 void sweep_prepare(qas_ctx *c)
 {
-  switch (c->scheme.odr) {
-    case 1: sweep_prepare_o<1>(c); break;
-    case 2: sweep_prepare_o<2>(c); break;
-    case 3: sweep_prepare_o<3>(c); break;
-    default: sweep_prepare_o<4>(c); break;
+  if (c->scheme.odr != 4) return;
+  switch (c->scheme.rmn) {
+    case 0: sweep_prepare_t<0>(c); break;
+    case 1: sweep_prepare_t<1>(c); break;
+    case 2: sweep_prepare_t<2>(c); break;
+    default: sweep_prepare_t<3>(c); break;
   }
 }
 
-template <int ODR, int RMN>
-void launch_sweep(qas_ctx *c, int a)
+template <int RMN, int PR>
+void launch_sweep_pr(qas_ctx *c, int a)
 {
   const Geo &g = c->geo;
   if (a == 0) {
@@ -560,18 +551,26 @@ void launch_sweep(qas_ctx *c, int a)
     const long long total = (long long)(g.nx - 4) * g.ny * g.nz;
     const long long nwarps = (total - 2) / 31 + 1;
     const unsigned nb = (unsigned)((nwarps + 3) / 4);
-    QL(c, KID_SWEEP, k_sweep_x<ODR, RMN><<<nb, 128, 0, c->stream>>>(c->view, nwarps));
+    QL(c, KID_SWEEP, k_sweep_x<4, RMN, PR><<<nb, 128, 0, c->stream>>>(c->view, nwarps));
     return;
   }
   const unsigned colb = (unsigned)(((long long)g.nx * (a == 1 ? g.nz : g.ny) + 127) / 128);
   const int len = g.n[a] - 5;
   if (a == 1) {
-    const int seg = sweep_seg(c, 1, (const void *)k_sweep_m<ODR, RMN, 1>);
-    QL(c, KID_SWEEP, k_sweep_m<ODR, RMN, 1><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
+    const int seg = sweep_seg(c, 1, (const void *)k_sweep_m<4, RMN, 1, 0>);
+    QL(c, KID_SWEEP, k_sweep_m<4, RMN, 1, PR><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
   } else {
-    const int seg = sweep_seg(c, 2, (const void *)k_sweep_m<ODR, RMN, 2>);
-    QL(c, KID_SWEEP, k_sweep_m<ODR, RMN, 2><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
+    const int seg = sweep_seg(c, 2, (const void *)k_sweep_m<4, RMN, 2, 0>);
+    QL(c, KID_SWEEP, k_sweep_m<4, RMN, 2, PR><<<dim3(colb, (len + seg - 1) / seg), 128, 0, c->stream>>>(c->view, seg));
   }
+}
+template <int RMN>
+void launch_sweep(qas_ctx *c, int a)
+{
+  if (c->view.recon != 2)
+    launch_sweep_pr<RMN, 0>(c, a);
+  else
+    launch_sweep_pr<RMN, -1>(c, a);
 }
 
 // HMHD1D::crcte on the by and bz fluxes (1D Hall driver with electron inertia), after the
@@ -625,15 +624,17 @@ long long stage_rest(qas_ctx *c, double c0, double c1)
   const Geo &g = c->geo;
   long long nk = 0;
   for (int a = 0; a < g.dim; a++) {
-    if (c->fused) {
-      switch (c->scheme.rmn) {
-        case 0: launch_sweep<ODR, 0>(c, a); break;
-        case 1: launch_sweep<ODR, 1>(c, a); break;
-        case 2: launch_sweep<ODR, 2>(c, a); break;
-        default: launch_sweep<ODR, 3>(c, a); break;
+    if constexpr (ODR == 4) {
+      if (c->fused) {
+        switch (c->scheme.rmn) {
+          case 0: launch_sweep<0>(c, a); break;
+          case 1: launch_sweep<1>(c, a); break;
+          case 2: launch_sweep<2>(c, a); break;
+          default: launch_sweep<3>(c, a); break;
+        }
+        nk += 1;
+        continue;
       }
-      nk += 1;
-      continue;
     }
     launch_lr<ODR>(c, a);
     switch (c->scheme.rmn) {

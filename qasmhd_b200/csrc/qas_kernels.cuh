@@ -499,7 +499,10 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) k_flux_mlau(View v)
 //    cell's right-face state waits in a shared-memory slot of the thread, not in
 //    registers, so the reconstruction and the Riemann solver do not hold it live.
 // Resident-block caps per Riemann solver: the reconstruction's 6 (80 registers),
-// Roe's 4 (its flux needs 128).
+// Roe's 4 (its flux needs 128).  PR: 0 the characteristic or primitive reconstruction by
+// v.recon (the default scheme), -1 also the Athena-type form, whose code raises the kernels'
+// register pressure (spills 156 -> 712 B).  Built for 4th-order interpolation (the other orders
+// take the two-kernel form).
 // ---------------------------------------------------------------------------
 #ifndef QAS_SWEEP_MINB
 #define QAS_SWEEP_MINB 6
@@ -509,7 +512,8 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) k_flux_mlau(View v)
 #endif
 #define QAS_SWEEP_MINB_OF(RMN) ((RMN) == 0 ? QAS_SWEEP_ROE_MINB : QAS_SWEEP_MINB)
 
-template <int ODR, int A>
+// PR: 0 the characteristic or primitive form by v.recon, -1 any of the three
+template <int ODR, int A, int PR>
 __device__ __forceinline__ void cell_states(const View &v, long long c, double vl[7], double vr[7], double ql[2],
                                             double qr[2])
 {
@@ -523,9 +527,9 @@ __device__ __forceinline__ void cell_states(const View &v, long long c, double v
   const double *cb = B == 0 ? v.cx : (B == 1 ? v.cy : v.cz);
   const double *ccp = C == 0 ? v.cx : (C == 1 ? v.cy : v.cz);
   const LrStencil<A> st{v, c, s};
-  if (v.recon == 1)
+  if (PR <= 0 && v.recon == 1)
     face_states_prim<ODR>(st, vl, vr);
-  else if (v.recon == 2)
+  else if (PR < 0 && v.recon == 2)
     face_states_athena<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
   else
     face_states_grouped<ODR>(st, __ldg(cn + c), v.gam, vl, vr);
@@ -582,12 +586,12 @@ __device__ __forceinline__ void face_flux(const View &v, long long f, const doub
 // past the end, have_cell false, so that the warp stays converged), the hand-off of the right-face
 // state to the next lane, and the flux at the cell's left face when the previous lane holds the
 // cell to its left (i >= 3)
-template <int ODR, int RMN>
+template <int ODR, int RMN, int PR>
 __device__ __forceinline__ void sweep_x_cell(const View &v, int i, int j, int k, int lane, bool have_cell)
 {
   const long long c = cidx(v.g, i, j, k);
   double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
-  cell_states<ODR, 0>(v, c, vl, vr, ql, qr);
+  cell_states<ODR, 0, PR>(v, c, vl, vr, ql, qr);
   double L[7], QL[2];
 #pragma unroll
   for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
@@ -597,7 +601,7 @@ __device__ __forceinline__ void sweep_x_cell(const View &v, int i, int j, int k,
 }
 
 // x sweep: 4 warps per block, 31 faces per warp over the flattened cells of all rows
-template <int ODR, int RMN>
+template <int ODR, int RMN, int PR>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_x(View v, long long nwarps)
 {
   if (v.ctl->done) return;
@@ -612,13 +616,22 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_x(View v,
   if (!have_cell) t = total - 1;  // a valid cell, computed and discarded (keeps the warp converged)
   const long long row = t / ncell;
   const int i = 2 + (int)(t - row * ncell);
-  sweep_x_cell<ODR, RMN>(v, i, (int)(row % g.ny), (int)(row / g.ny), lane, have_cell);
+  const long long c = cidx(g, i, (int)(row % g.ny), (int)(row / g.ny));
+  double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+  cell_states<ODR, 0, PR>(v, c, vl, vr, ql, qr);
+  double L[7], QL[2];
+#pragma unroll
+  for (int m = 0; m < 7; m++) L[m] = __shfl_up_sync(0xffffffffu, vl[m], 1);
+  QL[0] = __shfl_up_sync(0xffffffffu, ql[0], 1);
+  QL[1] = __shfl_up_sync(0xffffffffu, ql[1], 1);
+  // lane-1 holds cell i-1 of the same row exactly when i >= 3
+  if (lane >= 1 && have_cell && i >= 3) face_flux<RMN, 0>(v, c, L, vr, QL, qr);
 }
 
 // one column of a y / z sweep: the faces p in [p0, p1) along A of the column through (i, o)
 // (o = k for the y sweep, j for the z sweep), from the cell before p0 on; the previous cell's
 // right-face state waits in the thread's shared-memory slot carry[.][tid]
-template <int ODR, int RMN, int A>
+template <int ODR, int RMN, int A, int PR>
 __device__ __forceinline__ void sweep_column(const View &v, int i, int o, int p0, int p1, double (*carry)[128], int tid)
 {
   const Geo &g = v.g;
@@ -626,7 +639,7 @@ __device__ __forceinline__ void sweep_column(const View &v, int i, int o, int p0
   long long c = A == 1 ? cidx(g, i, p0 - 1, o) : cidx(g, i, o, p0 - 1);
   {
     double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
-    cell_states<ODR, A>(v, c, vl, vr, ql, qr);
+    cell_states<ODR, A, PR>(v, c, vl, vr, ql, qr);
 #pragma unroll
     for (int m = 0; m < 7; m++) carry[m][tid] = vl[m];
     carry[7][tid] = ql[0];
@@ -635,7 +648,7 @@ __device__ __forceinline__ void sweep_column(const View &v, int i, int o, int p0
   for (int p = p0; p < p1; p++) {
     c += s;
     double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
-    cell_states<ODR, A>(v, c, vl, vr, ql, qr);
+    cell_states<ODR, A, PR>(v, c, vl, vr, ql, qr);
     double L[7], QL[2];
 #pragma unroll
     for (int m = 0; m < 7; m++) {
@@ -651,7 +664,7 @@ __device__ __forceinline__ void sweep_column(const View &v, int i, int o, int p0
 }
 
 // y / z sweep: one thread per column, marching over `seg` faces along A
-template <int ODR, int RMN, int A>
+template <int ODR, int RMN, int A, int PR>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v, int seg)
 {
   if (v.ctl->done) return;
@@ -661,8 +674,35 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) k_sweep_m(View v,
   const int no = A == 1 ? g.nz : g.ny;  // extent of the other transverse axis
   const long long col = (long long)blockIdx.x * 128 + tid;
   if (col >= (long long)g.nx * no) return;  // no barrier below: threads leave freely
+  const int i = (int)(col % g.nx), o = (int)(col / g.nx);
   const int p0 = 3 + blockIdx.y * seg;
-  sweep_column<ODR, RMN, A>(v, (int)(col % g.nx), (int)(col / g.nx), p0, min(p0 + seg, g.n[A] - 2), carry, tid);
+  const int p1 = min(p0 + seg, g.n[A] - 2);
+  const long long s = g.s[A];
+  long long c = A == 1 ? cidx(g, i, p0 - 1, o) : cidx(g, i, o, p0 - 1);
+  {
+    double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+    cell_states<ODR, A, PR>(v, c, vl, vr, ql, qr);
+#pragma unroll
+    for (int m = 0; m < 7; m++) carry[m][tid] = vl[m];
+    carry[7][tid] = ql[0];
+    carry[8][tid] = ql[1];
+  }
+  for (int p = p0; p < p1; p++) {
+    c += s;
+    double vl[7], vr[7], ql[2] = {0.0, 0.0}, qr[2] = {0.0, 0.0};
+    cell_states<ODR, A, PR>(v, c, vl, vr, ql, qr);
+    double L[7], QL[2];
+#pragma unroll
+    for (int m = 0; m < 7; m++) {
+      L[m] = carry[m][tid];
+      carry[m][tid] = vl[m];
+    }
+    QL[0] = carry[7][tid];
+    QL[1] = carry[8][tid];
+    carry[7][tid] = ql[0];
+    carry[8][tid] = ql[1];
+    face_flux<RMN, A>(v, c, L, vr, QL, qr);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(128, QAS_FLUX_MLAU_MINB) kw_flux_mlau(View v, 
 
 // fused face sweeps on a window (the default form in 3D, see k_sweep_x / k_sweep_m)
 // x sweep over the flattened cells of the rows of planes r
-template <int ODR, int RMN>
+template <int ODR, int RMN, int PR>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_x(View v, Rows2 r, long long nwarps)
 {
   QAS_PDL_WAIT();
@@ -130,12 +130,12 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_x(View v
   const int i = 2 + (int)(t - row * ncell);
   const int j = g.dim == 3 ? (int)(row % g.ny) : rows2_plane(r, (int)row);
   const int k = g.dim == 3 ? rows2_plane(r, (int)(row / g.ny)) : 0;
-  sweep_x_cell<ODR, RMN>(v, i, j, k, lane, have_cell);
+  sweep_x_cell<ODR, RMN, PR>(v, i, j, k, lane, have_cell);
 }
 
 // y sweep of a 3D window (an in-plane axis): columns (i, k) with k on planes r, every y face
 // [3, ny-2) in segments of `seg`
-template <int ODR, int RMN>
+template <int ODR, int RMN, int PR>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_y3(View v, Rows2 r, int seg)
 {
   QAS_PDL_WAIT();
@@ -146,13 +146,13 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_y3(View 
   const long long col = (long long)blockIdx.x * 128 + tid;
   if (col >= (long long)g.nx * (rows_len(r.a) + rows_len(r.b))) return;
   const int p0 = 3 + blockIdx.y * seg;
-  sweep_column<ODR, RMN, 1>(v, (int)(col % g.nx), rows2_plane(r, (int)(col / g.nx)), p0, min(p0 + seg, g.ny - 2),
+  sweep_column<ODR, RMN, 1, PR>(v, (int)(col % g.nx), rows2_plane(r, (int)(col / g.nx)), p0, min(p0 + seg, g.ny - 2),
                             carry, tid);
 }
 
 // sweep along the last axis A (y in 2D, z in 3D): every column (i, j in 3D), the faces of
 // f = r clipped to [3, n-2), chunk q of `seg` faces per blockIdx.y: first those of r.a, then r.b
-template <int ODR, int RMN, int A>
+template <int ODR, int RMN, int A, int PR>
 __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_last(View v, Rows2 f, int seg)
 {
   QAS_PDL_WAIT();
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(128, QAS_SWEEP_MINB_OF(RMN)) kw_sweep_last(Vie
   const Rows &x = q < ca ? a : b;
   const int p0 = x.lo + (q < ca ? q : q - ca) * seg;
   if (p0 >= x.hi) return;
-  sweep_column<ODR, RMN, A>(v, (int)(col % g.nx), (int)(col / g.nx), p0, min(p0 + seg, x.hi), carry, tid);
+  sweep_column<ODR, RMN, A, PR>(v, (int)(col % g.nx), (int)(col / g.nx), p0, min(p0 + seg, x.hi), carry, tid);
 }
 
 template <int ODR>
