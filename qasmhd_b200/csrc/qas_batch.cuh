@@ -39,12 +39,14 @@ __device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, 
   }
 }
 
-// Block loop of a persistent batched kernel.  QAS_BATCH_CONTIGUOUS = 1: each CTA takes one
-// contiguous run of the (instance-major) block list, so its consecutive blocks share an
-// instance and that instance's View, control word and launch grid stay in L1; the next map
-// entry is loaded while the current block works.  0: grid-stride over the list.
+// Block loop of a persistent batched kernel.  0 (default): grid-stride over the block list.
+// QAS_BATCH_CONTIGUOUS = 1: each CTA takes one contiguous run of the (instance-major) list, so
+// that its consecutive blocks share an instance (View, control word and launch grid in L1), with
+// the next map entry loaded while the current block works -- measured slower on B200 (512-member
+// C4 ensemble: 551 against 587 Mcell-updates/s): the long runs of one instance per CTA balance
+// the SMs worse than the interleaved stride.
 #ifndef QAS_BATCH_CONTIGUOUS
-#define QAS_BATCH_CONTIGUOUS 1
+#define QAS_BATCH_CONTIGUOUS 0
 #endif
 #if QAS_BATCH_CONTIGUOUS
 #define QAS_BATCH_BLOCKS(map)                                                         \
