@@ -162,3 +162,35 @@ def test_kh_inversion_full_size():
         assert abs(fd - an) <= 1e-2 * abs(an)
     finally:
         P.close()
+
+
+def test_kh_inversion_full_size_vs_extended_precision_fd():
+    """C5 against central differences taken in extended precision: the reference's 2D stepping
+    code built in long double (oracle/_ref/ref2d_ld_ctw1), 32 seeded directions of the vy
+    perturbation (eps = 1e-6) and eta (step 1e-9), with the same frozen dt sequence and target
+    (tests/golden/c5_fd_longdouble.json, made by tests/golden/make_c5_fd.py).  The double-
+    precision differences above are quantised by the pressure recovery; these are not, so the
+    adjoint must match them to 1e-6 of the largest directional derivative, direction by
+    direction, and to 1e-6 relative on eta."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c5_fd_longdouble.json")
+    if not os.path.exists(path):
+        pytest.skip("tests/golden/c5_fd_longdouble.json not generated")
+    gold = json.load(open(path))
+    P = KHInverse(n=gold["n"], nsteps=gold["nsteps"], ckpt_every=20)
+    try:
+        assert np.array_equal(P.dts, np.array(gold["dts"]))  # the reference's exec_ dt sequence
+        dvy = np.random.default_rng(gold["dvy_seed"]).standard_normal((P.n, P.n))
+        x = torch.from_numpy(dvy).requires_grad_(True)
+        e = torch.tensor(gold["eta"], dtype=torch.float64, requires_grad=True)
+        loss = P.loss(x, e)
+        loss.backward()
+        assert abs(float(loss) - gold["loss"]) <= 1e-9 * gold["loss"]
+        rng = np.random.default_rng(gold["dir_seed"])
+        ads = np.array([float(np.sum(x.grad.numpy() * rng.standard_normal((P.n, P.n)))) for _ in gold["fd_dirs"]])
+        fds = np.array(gold["fd_dirs"])
+        assert np.max(np.abs(ads - fds)) <= 1e-6 * np.max(np.abs(fds)), np.max(np.abs(ads - fds)) / np.max(np.abs(fds))
+        assert abs(float(e.grad) - gold["fd_eta"]) <= 1e-6 * abs(gold["fd_eta"]), (float(e.grad), gold["fd_eta"])
+    finally:
+        P.close()
