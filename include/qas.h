@@ -301,9 +301,10 @@ qas_status qas_kernel_launches(const qas_ctx *ctx, long long *count);
  * Batched ensemble: many independent instances stepped by one set of kernel launches per
  * stage (one graph-captured launch sequence for the whole ensemble).  The reference runs
  * one simulation per process with a compile-time grid; this entry point has no counterpart
- * there beyond running many of its exec_() loops.  All instances share dim, ODR and R_K;
- * grid sizes, gamma, boundary flags, Riemann solver and CUCT flag are per instance.  Each
- * instance keeps its own dt (setdt every 2nd step), time and step counter.
+ * there beyond running many of its exec_() loops.  All instances share ODR and R_K; 2D and
+ * 3D instances may be mixed (1D instances only with 1D ones: QAS_ERR_INVALID otherwise); grid
+ * sizes, gamma, boundary flags, Riemann solver, CUCT flag and reconstruction are per instance.
+ * Each instance keeps its own dt (setdt every 2nd step), time and step counter.
  * ------------------------------------------------------------------------------------ */
 typedef struct qas_batch qas_batch;
 qas_status qas_batch_create(qas_batch **batch, int n, const qas_grid *grids, const qas_scheme *schemes,

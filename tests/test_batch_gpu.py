@@ -86,6 +86,34 @@ def test_batch_rejects_mixed_order():
     probs = [P.orszag_tang(16), P.orszag_tang(16, odr=2)]
     with pytest.raises(L.QasError):
         L.Batch(probs)
+    with pytest.raises(L.QasError):  # 1D instances run only with 1D ones
+        L.Batch([P.orszag_tang(16), P.brio_wu(64)])
+
+
+@pytest.mark.parametrize("tuned", [False, True])
+def test_batch_mixed_2d_3d(restatement, tuned):
+    """2D and 3D instances of uneven sizes in one ensemble (the face sweeps of z cover the 3D
+    instances only), each bit-identical to its own oracle run, with the default linear block maps
+    and after autotuning (tiles with a z extent leave the 2D instances' extra threads idle)."""
+    probs = [P.orszag_tang(24, nym=18),
+             P.kelvin_helmholtz(3, 8, mach=0.3, rmn=P.RMN_MLAU),
+             P.kelvin_helmholtz(2, 20, nym=16, mach=0.2, rmn=P.RMN_MLAU),
+             P.kelvin_helmholtz(3, 10, nym=8, nzm=12, mach=0.5, rmn=P.RMN_HLLD, seed=3),
+             P.smooth_wave(3, 6, rmn=P.RMN_ROE),
+             P.smooth_wave(2, 14, rmn=P.RMN_LHLLD)]
+    with L.Batch(probs) as b:
+        for q, p in enumerate(probs):
+            b.upload(q, p.state)
+        if tuned:
+            b.autotune(1)
+            for q, p in enumerate(probs):
+                b.upload(q, p.state)
+        info = b.run(max_steps=3, flg=1, stop_rule=0, cfl=0.4)
+        outs = [b.download(q, p.state.shape) for q, p in enumerate(probs)]
+    for q, p in enumerate(probs):
+        want = restatement.run(p, 3, mode=R.MODE_RUN)
+        assert info[q][2] == want["dt"], p.name
+        assert_bitwise(outs[q], want["state"], f"{p.name} ({p.dim}D)")
 
 
 def test_batch_mixed_reconstruction(restatement):
