@@ -13,9 +13,14 @@ moves `en` by tens of ulps); the 64-bit significand removes that floor.
 
 Inputs made here on the CPU from the reference's double build: the dt sequence (exec_ rule,
 setdt every second step, eta*) and the target observation (the reference's 400-step run from the
-target perturbation).  Writes tests/golden/c5_fd_longdouble.json.  ~1 hour on 8 cores:
+target perturbation).  Beside the differences the file holds the same directional derivatives
+from the reference's dual-number build (oracle/_ref/ref2d_dual_ctw1: the exact derivative of
+the double-precision program along each direction, `dual_dirs`, `dual_eta`).  Writes
+tests/golden/c5_fd_longdouble.json (other sizes: c5_fd_longdouble_<n>_<nsteps>_<ndir>.json).
+~2 hours on 8 cores at full size:
 
     python tests/golden/make_c5_fd.py [n nsteps ndir]     # defaults 256 400 32
+    python tests/golden/make_c5_fd.py --dual FILE         # (re)compute the dual fields of FILE
 """
 import json
 import os
@@ -65,7 +70,65 @@ def observe(u, n):
     return np.stack([u[1][s] / ro, u[2][s] / ro, u[4][s], u[5][s]])
 
 
+def dual_derivatives(gold, ndir=None):
+    """Directional derivatives of the loss along the golden's directions (the first ndir) and
+    eta from the reference's dual-number build, with the golden's dt sequence:
+    dL = 2 sum (obs - target) d(obs), d(vx) = d(mx)/ro - mx d(ro)/ro^2."""
+    n = gold["n"]
+    ndir = len(gold["fd_dirs"]) if ndir is None else ndir
+    threads = os.cpu_count()
+    base, amp = setup(n)
+    dts = np.array(gold["dts"])
+    ut = state(base, amp, np.random.default_rng(gold["target_seed"]).standard_normal((n, n)))
+    fin_t, _ = R.run_reference_dual(base, ut.reshape(8, -1), np.zeros((8, base.nd)), dts,
+                                    eta0=gold["eta_target"], nthreads=threads)
+    target = observe(fin_t.reshape(8, base.ny, base.nx), n)
+    u0 = state(base, amp, np.random.default_rng(gold["dvy_seed"]).standard_normal((n, n)))
+    ro = u0[0]
+    vy = u0[2] / ro
+    s = (slice(XOFF, XOFF + n), slice(XOFF, XOFF + n))
+    ampf = np.zeros_like(ro)
+    ampf[s] = amp
+    rng = np.random.default_rng(gold["dir_seed"])
+    tangents = []
+    for _ in range(ndir):
+        dd = np.zeros_like(ro)
+        dd[s] = rng.standard_normal((n, n))
+        t = np.zeros_like(u0)
+        t[2] = ro * ampf * dd  # d(my) for vy = amp * dvy
+        t[7] = ro * vy * ampf * dd  # d(en) = ro vy d(vy)
+        tangents.append((t, 0.0))
+    tangents.append((np.zeros_like(u0), 1.0))  # eta
+    out = []
+    for t, deta in tangents:
+        v, dv = R.run_reference_dual(base, u0.reshape(8, -1), t.reshape(8, -1), dts, eta0=gold["eta"],
+                                     deta=deta, nthreads=threads)
+        v = v.reshape(8, base.ny, base.nx)
+        dv = dv.reshape(8, base.ny, base.nx)
+        d = observe(v, n) - target
+        r, dr = v[0][s], dv[0][s]
+        dobs = np.stack([dv[1][s] / r - v[1][s] * dr / (r * r), dv[2][s] / r - v[2][s] * dr / (r * r),
+                         dv[4][s], dv[5][s]])
+        out.append(2.0 * float(np.sum(d * dobs)))
+    return out[:-1], out[-1]
+
+
+def add_dual(path):
+    gold = json.load(open(path))
+    t0 = time.time()
+    gold["dual_dirs"], gold["dual_eta"] = dual_derivatives(gold)
+    gold["dual_seconds"] = time.time() - t0
+    with open(path, "w") as f:
+        json.dump(gold, f, indent=1)
+    fd, du = np.array(gold["fd_dirs"]), np.array(gold["dual_dirs"])
+    print(path, "max |fd - dual| / max |fd| =", float(np.max(np.abs(fd - du)) / np.max(np.abs(fd))),
+          "eta", abs(gold["fd_eta"] - gold["dual_eta"]) / abs(gold["dual_eta"]))
+
+
 def main():
+    if len(sys.argv) > 2 and sys.argv[1] == "--dual":
+        add_dual(sys.argv[2])
+        return
     n, nsteps, ndir = (int(a) for a in (sys.argv[1:4] if len(sys.argv) > 3 else (256, 400, 32)))
     threads = os.cpu_count()
     base, amp = setup(n)
@@ -103,6 +166,7 @@ def main():
     with open(path, "w") as f:
         json.dump(res, f, indent=1)
     print(path, res["fd_dirs"][:3], res["fd_eta"], res["loss"], f"{res['seconds']:.0f} s")
+    add_dual(path)
 
 
 if __name__ == "__main__":

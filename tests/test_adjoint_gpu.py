@@ -164,19 +164,36 @@ def test_kh_inversion_full_size():
         P.close()
 
 
-def test_kh_inversion_full_size_vs_extended_precision_fd():
-    """C5 against central differences taken in extended precision: the reference's 2D stepping
-    code built in long double (oracle/_ref/ref2d_ld_ctw1), 32 seeded directions of the vy
-    perturbation (eps = 1e-6) and eta (step 1e-9), with the same frozen dt sequence and target
-    (tests/golden/c5_fd_longdouble.json, made by tests/golden/make_c5_fd.py).  The double-
-    precision differences above are quantised by the pressure recovery; these are not, so the
-    adjoint must match them to 1e-6 of the largest directional derivative, direction by
-    direction, and to 1e-6 relative on eta."""
+# (golden, tolerance of adjoint vs the long double differences, of max |fd|)
+FD_GOLDENS = [
+    # KH 32^2, 20 steps: differences and the reference's dual derivative agree to 7e-10
+    ("c5_fd_longdouble_32_20_2.json", 1e-6),
+    # C5 as specified (256^2, 400 steps): the differences' own floor, 1.85e-5 (see below)
+    ("c5_fd_longdouble.json", 3e-5),
+]
+
+
+@pytest.mark.parametrize("name,tol_fd", FD_GOLDENS, ids=[g[0] for g in FD_GOLDENS])
+def test_kh_inversion_vs_extended_precision_fd(name, tol_fd):
+    """The KH inversion gradient against central differences taken in extended precision: the
+    reference's 2D stepping code built in long double (oracle/_ref/ref2d_ld_ctw1), 32 seeded
+    directions of the vy perturbation (eps = 1e-6) and eta (step 1e-9), with the same frozen dt
+    sequence and target (tests/golden/c5_fd_longdouble*.json, made by tests/golden/make_c5_fd.py,
+    which also stores the reference's dual-number derivative along the same directions).
+
+    The adjoint must equal the reference's dual derivative (the exact derivative of the same
+    double-precision program) to 1e-9, direction by direction, and lie no farther from the
+    differences than that derivative does.  On the full C5 run the differences themselves stop
+    at 1.85e-5 of the largest directional derivative (dual and adjoint alike; eta 3.5e-8): the
+    loss is not smooth at the scale of the step -- Roe's |vn| eigenvalues cross zero inside
+    the step in some directions (the worst one falls 40x with eps = 1e-8) and some branches are
+    tied at the base point, where central differences average the two one-sided derivatives
+    (2-3.5e-6 whatever the step).  On the 20-step 32^2 run they agree to 7e-10."""
     import json
     import os
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c5_fd_longdouble.json")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name)
     if not os.path.exists(path):
-        pytest.skip("tests/golden/c5_fd_longdouble.json not generated")
+        pytest.skip(f"tests/golden/{name} not generated")
     gold = json.load(open(path))
     P = KHInverse(n=gold["n"], nsteps=gold["nsteps"], ckpt_every=20)
     try:
@@ -186,11 +203,16 @@ def test_kh_inversion_full_size_vs_extended_precision_fd():
         e = torch.tensor(gold["eta"], dtype=torch.float64, requires_grad=True)
         loss = P.loss(x, e)
         loss.backward()
-        assert abs(float(loss) - gold["loss"]) <= 1e-9 * gold["loss"]
+        assert abs(float(loss.detach()) - gold["loss"]) <= 1e-9 * gold["loss"]
         rng = np.random.default_rng(gold["dir_seed"])
         ads = np.array([float(np.sum(x.grad.numpy() * rng.standard_normal((P.n, P.n)))) for _ in gold["fd_dirs"]])
-        fds = np.array(gold["fd_dirs"])
-        assert np.max(np.abs(ads - fds)) <= 1e-6 * np.max(np.abs(fds)), np.max(np.abs(ads - fds)) / np.max(np.abs(fds))
-        assert abs(float(e.grad) - gold["fd_eta"]) <= 1e-6 * abs(gold["fd_eta"]), (float(e.grad), gold["fd_eta"])
+        geta = float(e.grad)
+        fds, dus = np.array(gold["fd_dirs"]), np.array(gold["dual_dirs"])
+        scale = np.max(np.abs(fds))
+        assert np.max(np.abs(ads - dus)) <= 1e-9 * np.max(np.abs(dus)), np.max(np.abs(ads - dus)) / np.max(np.abs(dus))
+        assert abs(geta - gold["dual_eta"]) <= 1e-9 * abs(gold["dual_eta"]), (geta, gold["dual_eta"])
+        assert np.max(np.abs(ads - fds)) <= np.max(np.abs(dus - fds)) + 1e-9 * scale
+        assert np.max(np.abs(ads - fds)) <= tol_fd * scale, np.max(np.abs(ads - fds)) / scale
+        assert abs(geta - gold["fd_eta"]) <= 1e-6 * abs(gold["fd_eta"]), (geta, gold["fd_eta"])
     finally:
         P.close()
