@@ -168,6 +168,8 @@ def test_kh_inversion_full_size():
 FD_GOLDENS = [
     # KH 32^2, 20 steps: differences and the reference's dual derivative agree to 7e-10
     ("c5_fd_longdouble_32_20_2.json", 1e-6),
+    # the C5 problem at full resolution over its first 40 steps: they agree to 5.3e-10
+    ("c5_fd_longdouble_256_40_32.json", 1e-6),
     # C5 as specified (256^2, 400 steps): the differences' own floor, 1.85e-5 (see below)
     ("c5_fd_longdouble.json", 3e-5),
 ]
@@ -188,7 +190,9 @@ def test_kh_inversion_vs_extended_precision_fd(name, tol_fd):
     loss is not smooth at the scale of the step -- Roe's |vn| eigenvalues cross zero inside
     the step in some directions (the worst one falls 40x with eps = 1e-8) and some branches are
     tied at the base point, where central differences average the two one-sided derivatives
-    (2-3.5e-6 whatever the step).  On the 20-step 32^2 run they agree to 7e-10."""
+    (2-3.5e-6 whatever the step).  On the 20-step 32^2 run they agree to 7e-10, and on the C5
+    problem at full resolution over 40 steps to 5.3e-10 (eta 4.5e-10): there the adjoint is held
+    to 1e-6 of central FD."""
     import json
     import os
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name)
