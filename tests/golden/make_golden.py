@@ -64,6 +64,26 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
         a[3::7, 25:30] = 0.0      # exactly-zero bu stencils
         a[5::11, 5:10] *= 8.0     # supersonic centres (fast-mode eigenvectors)
         return a
+    if kind == "lrstate_vac":
+        # near-vacuum stencils: density and / or pressure falling to 1e-16..1e-10 across the
+        # stencil, so that reconstructed face values reach the positivity fallback of
+        # mhd_lrstate (common/mhd_func.c:150-160: first order when rho or p <= 1e-12)
+        ro = np.repeat(rng.uniform(0.5, 2.0, (n, 1)), 5, axis=1)
+        pr = np.repeat(rng.uniform(0.5, 2.0, (n, 1)), 5, axis=1)
+        tiny = 10.0 ** rng.uniform(-16, -10, n)
+        for r in range(n):
+            k = r % 4
+            if k == 0:
+                ro[r, 3:] = tiny[r]
+            elif k == 1:
+                pr[r, 3:] = tiny[r]
+            elif k == 2:
+                ro[r, :2] = tiny[r]
+            else:
+                pr[r, :2] = tiny[r]
+                ro[r, 3:] = tiny[r]
+        rest = rng.normal(0, 1, (n, 25))
+        return np.concatenate([ro, rest, pr, rng.normal(0, 1, (n, 1)), np.full((n, 1), 5.0 / 3.0)], axis=1)
     if kind == "cuct":
         return np.concatenate([np.abs(rng.normal(1, 0.2, (n, 4))) + 0.1, rng.normal(0, 1, (n, 16))], axis=1)
     if kind == "energy":
@@ -81,6 +101,7 @@ def kat_inputs(kind: str, n: int = 200, seed: int = 2024) -> np.ndarray:
 
 KAT_FUNCS = {"flux": ([0, 1, 2, 3], 7), "interp": (list(range(10, 20)), 2), "lrstate": ([20, 21, 22, 23], 14),
              "lrstate_prim": ([24, 25, 26, 27], 14), "lrstate_char": ([40, 41, 42, 43], 14), "cuct": ([30], 1),
+             "lrstate_vac": ([20, 21, 22, 23], 14),
              "energy": ([31, 32], 1)}
 
 
