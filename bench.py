@@ -2,8 +2,9 @@
 
 Default workload (N=1): 3D low-Mach Kelvin-Helmholtz 256^3 (M = 0.01, beta = 100),
 MLAU flux + characteristic WCNS4 + CUCT-weighted CT + SSP-RK3, CFL 0.4, dt refreshed
-every 2nd step as in exec_ -- the largest single-GPU configuration and the one the
-plain FP64 path is judged on.  One "step" = one full RK3 time step of the whole grid.
+every 2nd step as in exec_ -- the largest single-GPU configuration of the benchmark set
+and the one the throughput target of the plain FP64 path is stated on.  One "step" = one
+full RK3 time step of the whole grid.
 The timed region is K steps; it is timed `--windows` times and the median window is
 the reported value.  Under torchrun (N>1) every rank advances its own independent
 replica (the plain path is a single domain; replicas only), so per-GPU work is
