@@ -127,6 +127,15 @@ qas_status qas_primitives(qas_ctx *ctx, double *prim[4], double *cc[3]);
 /* Same with one contiguous host block of 8*nd doubles (field m at block + m*nd). */
 qas_status qas_upload_block(qas_ctx *ctx, const double *block);
 qas_status qas_download_block(qas_ctx *ctx, double *block);
+/* Asynchronous forms: the eight copies are queued on the context's stream behind the work
+ * already there and the call returns without waiting; later calls on the context are ordered
+ * after them.  The host block must stay valid -- and, for an upload, unchanged -- until
+ * qas_sync returns; a download's values are there only then.  With pinned host memory
+ * (cudaHostAlloc) the copies overlap the caller's host work; with pageable memory the driver
+ * may finish them before the call returns.  The synchronous forms above are these plus
+ * qas_sync. */
+qas_status qas_upload_block_async(qas_ctx *ctx, const double *block);
+qas_status qas_download_block_async(qas_ctx *ctx, double *block);
 /* Device address of the context's state block (8*nd doubles, field-major); valid until
  * qas_destroy.  Lets device-resident callers (CUDA, PyTorch) share the state without copies. */
 qas_status qas_device_state(qas_ctx *ctx, double **d_block);

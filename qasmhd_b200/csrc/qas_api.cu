@@ -1113,6 +1113,24 @@ qas_status qas_download_block(qas_ctx *c, double *block)
   return qas_download(c, val);
 }
 
+qas_status qas_upload_block_async(qas_ctx *c, const double *block)
+{
+  if (!c || !block) return QAS_ERR_INVALID;
+  const size_t n = (size_t)c->geo.nd;
+  for (int m = 0; m < 8; m++)
+    QAS_CUDA(cudaMemcpyAsync(c->view.u[m], block + m * n, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return QAS_OK;
+}
+
+qas_status qas_download_block_async(qas_ctx *c, double *block)
+{
+  if (!c || !block) return QAS_ERR_INVALID;
+  const size_t n = (size_t)c->geo.nd;
+  for (int m = 0; m < 8; m++)
+    QAS_CUDA(cudaMemcpyAsync(block + m * n, c->view.u[m], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return QAS_OK;
+}
+
 qas_status qas_device_state(qas_ctx *c, double **d_block)
 {
   if (!c || !d_block) return QAS_ERR_INVALID;

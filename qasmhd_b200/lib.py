@@ -31,6 +31,7 @@ QAS_ERR_IO = 8
 EXPORTS = (
     "qas_status_str", "qas_abi_version", "qas_last_cuda_error", "qas_create", "qas_destroy",
     "qas_cells", "qas_upload", "qas_download", "qas_upload_block", "qas_download_block",
+    "qas_upload_block_async", "qas_download_block_async",
     "qas_device_state", "qas_stream", "qas_bound", "qas_step", "qas_cfl_vmax", "qas_cfl_dt",
     "qas_run", "qas_run_reset", "qas_step_host", "qas_pipe_plan", "qas_dissipate", "qas_dsptv", "qas_max_divb", "qas_sync",
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
@@ -125,6 +126,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_download.argtypes = [vp, ctypes.POINTER(dp)]
     lib.qas_upload_block.argtypes = [vp, dp]
     lib.qas_download_block.argtypes = [vp, dp]
+    lib.qas_upload_block_async.argtypes = [vp, dp]
+    lib.qas_download_block_async.argtypes = [vp, dp]
     lib.qas_device_state.argtypes = [vp, ctypes.POINTER(dp)]
     lib.qas_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.qas_bound.argtypes = [vp]
@@ -319,6 +322,18 @@ class Context:
         """Download into a caller-owned C-contiguous float64 buffer of 8*nd values (e.g. pinned)."""
         assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == 8 * self.nd
         _check(self.lib.qas_download_block(self.h, _dptr(out)), "qas_download_block")
+
+    def upload_async(self, state: np.ndarray) -> None:
+        """Queue the upload of a C-contiguous float64 block of 8*nd values (best pinned) on the
+        context's stream; `state` must stay alive and unchanged until sync()."""
+        assert state.dtype == np.float64 and state.flags["C_CONTIGUOUS"] and state.size == 8 * self.nd
+        _check(self.lib.qas_upload_block_async(self.h, _dptr(state)), "qas_upload_block_async")
+
+    def download_async(self, out: np.ndarray) -> None:
+        """Queue the download of the state into `out` (8*nd float64 values, best pinned); the
+        values are there after sync()."""
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == 8 * self.nd
+        _check(self.lib.qas_download_block_async(self.h, _dptr(out)), "qas_download_block_async")
 
     def upload_fields(self, fields: Sequence[np.ndarray]) -> None:
         """Upload 8 separate host arrays (the reference's val[8] pointers)."""

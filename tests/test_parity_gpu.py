@@ -125,6 +125,26 @@ def test_run_in_pieces_matches_one_call(restatement):
     assert_bitwise(out, a["state"], "pieces")
 
 
+def test_async_block_copies(restatement):
+    """qas_upload_block_async / qas_download_block_async from pinned host blocks: queued in stream
+    order behind the run, the state read back after qas_sync equals the oracle's 4-step result,
+    and an upload queued behind a download does not disturb what the download reads."""
+    import torch
+    p = P.orszag_tang(32)
+    a = restatement.run(p, 4, mode=R.MODE_RUN)
+    with L.Context.from_problem(p) as ctx:
+        up = torch.empty(8 * ctx.nd, dtype=torch.float64, pin_memory=True).numpy()
+        up[:] = p.state.reshape(-1)
+        down = torch.empty(8 * ctx.nd, dtype=torch.float64, pin_memory=True).numpy()
+        ctx.upload_async(up)
+        ctx.run(max_steps=4, flg=1, stop_rule=0, cfl=p.cfl)
+        ctx.download_async(down)
+        ctx.upload_async(up)  # restores the initial state after the download in stream order
+        ctx.sync()
+        assert_bitwise(down.reshape(p.state.shape), a["state"], "async round trip")
+        assert_bitwise(ctx.download(p.state.shape), p.state, "upload after download")
+
+
 def test_cfl_reduction_matches(restatement):
     p = P.kelvin_helmholtz(3, 12, mach=0.4)
     import ctypes
