@@ -36,12 +36,14 @@ typedef enum {
   QAS_OK = 0,
   QAS_ERR_INVALID = 1,      /* bad argument (sizes, flags, null pointers)            */
   QAS_ERR_CUDA = 2,         /* CUDA runtime error (see qas_last_cuda_error)          */
-  QAS_ERR_NOMEM = 3,        /* device allocation failed                              */
+  QAS_ERR_NOMEM = 3,        /* device (or host) allocation failed                    */
   QAS_ERR_NONFINITE = 4,    /* device check found rho<=0, p<=0 or a non-finite value */
   QAS_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up                    */
   QAS_ERR_UNSUPPORTED = 6,  /* combination not implemented                           */
   QAS_ERR_NO_DEVICE = 7,    /* no usable CUDA device                                 */
-  QAS_ERR_IO = 8            /* a file could not be written or read (message: qas_last_cuda_error) */
+  QAS_ERR_IO = 8,           /* a file could not be written or read (message: qas_last_cuda_error) */
+  QAS_ERR_HOST = 9          /* an exception in the library's host code, stopped at the C-ABI
+                               (message: qas_last_cuda_error); no exception crosses the ABI */
 } qas_status;
 
 /* Grid: compile-time XMESH/YMESH/ZMESH of mymacros.hpp plus paras()'s spacing and gamma

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <new>
 #include <string>
@@ -46,6 +47,32 @@ qas_status cuda_fail(cudaError_t e, const char *what)
   } while (0)
 
 double hmin(double a, double b) { return (a >= b) ? b : a; }  // common/common_func.h:11-15
+
+// No C++ exception crosses the C-ABI: every entry point's body runs inside QAS_API_TRY /
+// QAS_API_CATCH, which turn a failed host allocation into QAS_ERR_NOMEM and any other exception
+// of the host code (a thread the file writer could not start, ...) into QAS_ERR_HOST, with the
+// message kept for qas_last_cuda_error.
+qas_status host_fail(qas_status s, const char *what) noexcept
+{
+  try {
+    g_last_cuda_error = std::string("host exception: ") + what;
+  } catch (...) {
+  }
+  return s;
+}
+
+#define QAS_API_TRY try {
+#define QAS_API_CATCH                                                               \
+  }                                                                                 \
+  catch (const std::bad_alloc &) {                                                  \
+    return host_fail(QAS_ERR_NOMEM, "host memory allocation failed");               \
+  }                                                                                 \
+  catch (const std::exception &e_) {                                                \
+    return host_fail(QAS_ERR_HOST, e_.what());                                      \
+  }                                                                                 \
+  catch (...) {                                                                     \
+    return host_fail(QAS_ERR_HOST, "unknown exception");                            \
+  }
 
 }  // namespace
 
@@ -881,12 +908,13 @@ const char *qas_status_str(qas_status s)
     case QAS_OK: return "ok";
     case QAS_ERR_INVALID: return "invalid argument";
     case QAS_ERR_CUDA: return "CUDA error";
-    case QAS_ERR_NOMEM: return "out of device memory";
+    case QAS_ERR_NOMEM: return "out of memory";
     case QAS_ERR_NONFINITE: return "non-finite or non-positive state detected on the device";
     case QAS_ERR_TIMEOUT: return "bounded device wait timed out";
     case QAS_ERR_UNSUPPORTED: return "unsupported configuration";
     case QAS_ERR_NO_DEVICE: return "no CUDA device";
     case QAS_ERR_IO: return "file I/O failed";
+    case QAS_ERR_HOST: return "exception in the library's host code";
   }
   return "unknown status";
 }
@@ -897,6 +925,7 @@ const char *qas_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
 
 qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *scheme, const qas_bc *bc, int device)
 {
+  QAS_API_TRY
   if (!out || !grid || !scheme || !bc) return QAS_ERR_INVALID;
   *out = nullptr;
   const qas_grid &gr = *grid;
@@ -1014,10 +1043,12 @@ qas_status qas_create(qas_ctx **out, const qas_grid *grid, const qas_scheme *sch
   if ((st = write_ctl(c)) != QAS_OK) return fail(st);
   *out = c;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_destroy(qas_ctx *c)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (c->stream) cudaStreamSynchronize(c->stream);
   adj_free(c);
@@ -1040,17 +1071,21 @@ qas_status qas_destroy(qas_ctx *c)
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_cells(const qas_ctx *c, long long *nd)
 {
+  QAS_API_TRY
   if (!c || !nd) return QAS_ERR_INVALID;
   *nd = c->geo.nd;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_upload(qas_ctx *c, double *const val[8])
 {
+  QAS_API_TRY
   if (!c || !val) return QAS_ERR_INVALID;
   const size_t bytes = (size_t)c->geo.nd * sizeof(double);
   for (int m = 0; m < 8; m++) {
@@ -1059,10 +1094,12 @@ qas_status qas_upload(qas_ctx *c, double *const val[8])
   }
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_download(qas_ctx *c, double *val[8])
 {
+  QAS_API_TRY
   if (!c || !val) return QAS_ERR_INVALID;
   const size_t bytes = (size_t)c->geo.nd * sizeof(double);
   for (int m = 0; m < 8; m++) {
@@ -1071,10 +1108,12 @@ qas_status qas_download(qas_ctx *c, double *val[8])
   }
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_primitives(qas_ctx *c, double *prim[4], double *cc[3])
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   const Geo &g = c->geo;
   const dim3 t = c->tile[KID_PRIM];
@@ -1095,79 +1134,97 @@ qas_status qas_primitives(qas_ctx *c, double *prim[4], double *cc[3])
   }
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_upload_block(qas_ctx *c, const double *block)
 {
+  QAS_API_TRY
   if (!c || !block) return QAS_ERR_INVALID;
   double *val[8];
   for (int m = 0; m < 8; m++) val[m] = (double *)block + (size_t)m * c->geo.nd;
   return qas_upload(c, val);
+  QAS_API_CATCH
 }
 
 qas_status qas_download_block(qas_ctx *c, double *block)
 {
+  QAS_API_TRY
   if (!c || !block) return QAS_ERR_INVALID;
   double *val[8];
   for (int m = 0; m < 8; m++) val[m] = block + (size_t)m * c->geo.nd;
   return qas_download(c, val);
+  QAS_API_CATCH
 }
 
 qas_status qas_upload_block_async(qas_ctx *c, const double *block)
 {
+  QAS_API_TRY
   if (!c || !block) return QAS_ERR_INVALID;
   const size_t n = (size_t)c->geo.nd;
   for (int m = 0; m < 8; m++)
     QAS_CUDA(cudaMemcpyAsync(c->view.u[m], block + m * n, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_download_block_async(qas_ctx *c, double *block)
 {
+  QAS_API_TRY
   if (!c || !block) return QAS_ERR_INVALID;
   const size_t n = (size_t)c->geo.nd;
   for (int m = 0; m < 8; m++)
     QAS_CUDA(cudaMemcpyAsync(block + m * n, c->view.u[m], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_device_state(qas_ctx *c, double **d_block)
 {
+  QAS_API_TRY
   if (!c || !d_block) return QAS_ERR_INVALID;
   // the state arrays are consecutive in the pool with a 256-byte aligned stride; callers
   // that need a dense block use qas_upload_block / qas_download_block
   *d_block = c->view.u[0];
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_stream(qas_ctx *c, void **stream)
 {
+  QAS_API_TRY
   if (!c || !stream) return QAS_ERR_INVALID;
   *stream = (void *)c->stream;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_bound(qas_ctx *c)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_bound<<<shell_grid(c->geo), BLK, 0, c->stream>>>(c->view);
   c->launches++;
   return check_launch(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_step(qas_ctx *c, double dt)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   // a single ideal(dt): make sure the loop's done flag does not mask the kernels
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
   c->launches += 1 + launch_ideal(c);
   return check_launch(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_cfl_vmax(qas_ctx *c, double *vmax)
 {
+  QAS_API_TRY
   if (!c || !vmax) return QAS_ERR_INVALID;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   k_vmax_reset<<<1, 1, 0, c->stream>>>(c->view);
@@ -1180,27 +1237,33 @@ qas_status qas_cfl_vmax(qas_ctx *c, double *vmax)
   unsigned long long b = c->h_ctl->vmax_bits;
   memcpy(vmax, &b, sizeof(double));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_cfl_dt(qas_ctx *c, double cfl, double *dt)
 {
+  QAS_API_TRY
   if (!dt) return QAS_ERR_INVALID;
   double vmax = 0.0;
   qas_status s = qas_cfl_vmax(c, &vmax);
   if (s != QAS_OK) return s;
   *dt = cfl * c->dr / vmax;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_run_reset(qas_ctx *c)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   c->run_initialised = false;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
 {
+  QAS_API_TRY
   if (!c || !opts) return QAS_ERR_INVALID;
   qas_run_opts o = *opts;
   if (o.stop_rule < 0 || o.stop_rule > 2) return QAS_ERR_INVALID;
@@ -1295,10 +1358,12 @@ qas_status qas_run(qas_ctx *c, const qas_run_opts *opts, qas_run_info *info)
     info->dt = c->h_ctl->dt;
   }
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
   if (diss_arrays(c) && (nu0 != 0.0 || eta0 != 0.0)) return QAS_ERR_INVALID;
@@ -1334,10 +1399,12 @@ qas_status qas_dsptv(qas_ctx *c, double dt, double nu0, double eta0)
   }
   c->launches += nk;
   return check_launch(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
   if (diss_arrays(c) && (nu0 != 0.0 || eta0 != 0.0)) return QAS_ERR_INVALID;
@@ -1345,10 +1412,12 @@ qas_status qas_dissipate(qas_ctx *c, double dt, double nu0, double eta0)
   k_set_dt<<<1, 1, 0, c->stream>>>(c->view, dt);
   c->launches += 1 + launch_dissipate(c, nu0, eta0);
   return check_launch(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_max_divb(qas_ctx *c, double *maxdivb)
 {
+  QAS_API_TRY
   if (!c || !maxdivb) return QAS_ERR_INVALID;
   if (c->grid.dim < 2) {
     *maxdivb = 0.0;
@@ -1369,18 +1438,22 @@ qas_status qas_max_divb(qas_ctx *c, double *maxdivb)
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   memcpy(maxdivb, &bits, sizeof(double));
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_sync(qas_ctx *c)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   QAS_CUDA(cudaStreamSynchronize(c->stream));
   return read_ctl(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int field, int axis, int *src,
                       double *fac, int n)
 {
+  QAS_API_TRY
   if (!grid || !bc || !src || !fac) return QAS_ERR_INVALID;
   if (group < 0 || group > 3 || field < 0 || field >= (group == 0 ? 8 : 3) || axis < 0 || axis > 2)
     return QAS_ERR_INVALID;
@@ -1394,11 +1467,13 @@ qas_status qas_bc_map(const qas_grid *grid, const qas_bc *bc, int group, int fie
     fac[i] = m.fac[i];
   }
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas_kernel_time *out,
                            int max_entries, int *count)
 {
+  QAS_API_TRY
   if (!c || !opts || !out || !count || nsteps <= 0) return QAS_ERR_INVALID;
   qas_run_opts o = *opts;
   o.use_graph = 0;
@@ -1450,10 +1525,12 @@ qas_status qas_profile_run(qas_ctx *c, const qas_run_opts *opts, int nsteps, qas
   }
   *count = w;
   return read_ctl(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_set_dissipation(qas_ctx *c, const double *nu, const double *eta)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2 || c->view.phi) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaStreamSynchronize(c->stream));
@@ -1489,10 +1566,12 @@ qas_status qas_set_dissipation(qas_ctx *c, const double *nu, const double *eta)
   c->view.eta = c->d_eta;
   c->diss_dcmax = dcmax;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_set_hall(qas_ctx *c, double di, double de)
 {
+  QAS_API_TRY
   if (!c || !(di >= 0.0) || !(de >= 0.0)) return QAS_ERR_INVALID;
   if (c->grid.dim != 1) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaStreamSynchronize(c->stream));
@@ -1517,19 +1596,23 @@ qas_status qas_set_hall(qas_ctx *c, double di, double de)
   c->hall_de = de;
   c->hall_vphix = di * kpeak;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_hall(qas_ctx *c, double dt)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (!c->hall) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaMemsetAsync(&c->d_ctl->done, 0, sizeof(int), c->stream));
   c->launches += launch_hall(c, dt);
   return check_launch(c);
+  QAS_API_CATCH
 }
 
 qas_status qas_set_gravity(qas_ctx *c, const double *phi_g)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (c->grid.dim < 2) return QAS_ERR_UNSUPPORTED;
   QAS_CUDA(cudaStreamSynchronize(c->stream));
@@ -1550,10 +1633,12 @@ qas_status qas_set_gravity(qas_ctx *c, const double *phi_g)
   c->view.phi = c->d_phi;
   c->view.gfac = (2.0 - c->grid.gam) / (c->grid.gam - 1.0);  // fac of the drivers' bound()
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_set_option(qas_ctx *c, int option, int value)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   if (option == QAS_OPT_FUSED_SWEEP) {
     const bool f = value != 0;
@@ -1593,6 +1678,7 @@ qas_status qas_set_option(qas_ctx *c, int option, int value)
   if (option == QAS_OPT_PIPE_ITEMS) return pipe_set_items(c, value);
   if (option == QAS_OPT_PIPE_LANES) return pipe_set_lanes(c, value);
   return QAS_ERR_INVALID;
+  QAS_API_CATCH
 }
 
 static int tile_kid(const char *k)
@@ -1616,6 +1702,7 @@ static void drop_graph(qas_ctx *c)
 
 qas_status qas_set_tile(qas_ctx *c, const char *kernel, int tx, int ty, int tz)
 {
+  QAS_API_TRY
   if (!c) return QAS_ERR_INVALID;
   const int kid = tile_kid(kernel);
   if (kid == -2 || tx < 32 || tx % 32 || ty < 1 || tz < 1 || tx * ty * tz > 128) return QAS_ERR_INVALID;
@@ -1629,10 +1716,12 @@ qas_status qas_set_tile(qas_ctx *c, const char *kernel, int tx, int ty, int tz)
     c->tile[kid] = t;
   }
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_get_tile(const qas_ctx *c, const char *kernel, int *tx, int *ty, int *tz)
 {
+  QAS_API_TRY
   if (!c || !tx || !ty || !tz) return QAS_ERR_INVALID;
   const int kid = tile_kid(kernel);
   if (kid < 0) return QAS_ERR_INVALID;
@@ -1640,6 +1729,7 @@ qas_status qas_get_tile(const qas_ctx *c, const char *kernel, int *tx, int *ty, 
   *ty = c->tile[kid].y;
   *tz = c->tile[kid].z;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 namespace {
@@ -1660,6 +1750,7 @@ std::mutex g_tune_mu;
 
 qas_status qas_autotune(qas_ctx *c, int trial_steps)
 {
+  QAS_API_TRY
   if (!c || trial_steps <= 0) return QAS_ERR_INVALID;
   const int kids[6] = {KID_PRIM, KID_DV, KID_LR, KID_FLUX, KID_EMF, KID_UPDATE};
   int bucket = 0;
@@ -1738,10 +1829,12 @@ qas_status qas_autotune(qas_ctx *c, int trial_steps)
   for (int q = 0; q < 6; q++) e.tiles[q] = best[q];
   g_tune_cache.push_back(e);
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_fp64_peak(double *tflops)
 {
+  QAS_API_TRY
   if (!tflops) return QAS_ERR_INVALID;
   int dev = 0, sms = 0;
   QAS_CUDA(cudaGetDevice(&dev));
@@ -1765,13 +1858,16 @@ qas_status qas_fp64_peak(double *tflops)
   if (e != cudaSuccess) return cuda_fail(e, "fp64 peak");
   *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (ms * 1e-3) / 1e12;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 qas_status qas_kernel_launches(const qas_ctx *c, long long *count)
 {
+  QAS_API_TRY
   if (!c || !count) return QAS_ERR_INVALID;
   *count = c->launches;
   return QAS_OK;
+  QAS_API_CATCH
 }
 
 }  // extern "C"

@@ -26,6 +26,7 @@ QAS_ERR_TIMEOUT = 5
 QAS_ERR_UNSUPPORTED = 6
 QAS_ERR_NO_DEVICE = 7
 QAS_ERR_IO = 8
+QAS_ERR_HOST = 9
 
 # every exported entry point of include/qas.h (checked by the CPU tests)
 EXPORTS = (
@@ -204,7 +205,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
 def _check(status: int, what: str) -> None:
     if status != QAS_OK:
         detail = ""
-        if status in (QAS_ERR_CUDA, QAS_ERR_NOMEM, QAS_ERR_IO) and _lib is not None:
+        if status in (QAS_ERR_CUDA, QAS_ERR_NOMEM, QAS_ERR_IO, QAS_ERR_HOST) and _lib is not None:
             detail = _lib.qas_last_cuda_error().decode()
         raise QasError(status, what, detail)
 

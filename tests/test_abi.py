@@ -31,9 +31,40 @@ def test_library_exports_every_declared_symbol():
 
 def test_status_strings():
     lib = L.load()
-    for s in range(8):
-        assert lib.qas_status_str(s)
+    for s in range(10):
+        assert lib.qas_status_str(s) != b"unknown status"
     assert lib.qas_status_str(99) == b"unknown status"
+
+
+_NO_THROW = r"""
+import ctypes, resource, sys
+import numpy as np
+from qasmhd_b200 import lib as L
+lib = L.load()
+n = 50_000_000
+src = np.zeros(n, dtype=np.int32)
+fac = np.zeros(n, dtype=np.float64)
+g = L.Grid(1, n - 8, 1, 1, 1e-3, 0.0, 0.0, 5.0 / 3.0)
+bc = L.BC()
+vm = [int(l.split()[1]) * 1024 for l in open("/proc/self/status") if l.startswith("VmSize")][0]
+resource.setrlimit(resource.RLIMIT_AS, (vm + (200 << 20), resource.RLIM_INFINITY))
+st = lib.qas_bc_map(ctypes.byref(g), ctypes.byref(bc), 0, 0, 0,
+                    src.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                    fac.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n)
+print(st, lib.qas_last_cuda_error().decode())
+"""
+
+
+def test_no_exception_crosses_the_abi():
+    """A host allocation that fails inside an entry point (qas_bc_map's 600 MB of maps under a
+    200 MB address-space headroom) comes back as QAS_ERR_NOMEM with a message instead of an
+    exception crossing the C-ABI (which would end the process)."""
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, "-c", _NO_THROW], capture_output=True, text=True, cwd=ROOT, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    status, msg = r.stdout.strip().split(" ", 1)
+    assert int(status) == L.QAS_ERR_NOMEM and "host memory allocation failed" in msg, r.stdout
 
 
 def _has_gpu():
