@@ -145,6 +145,37 @@ def test_async_block_copies(restatement):
         assert_bitwise(ctx.download(p.state.shape), p.state, "upload after download")
 
 
+def test_contexts_on_host_threads(restatement):
+    """Distinct contexts are independent: four contexts (2D and 3D, different solvers) stepped at
+    the same time from four host threads (ctypes releases the GIL during each call) give the
+    oracle's results bit for bit."""
+    import threading
+    probs = [P.orszag_tang(32), P.kelvin_helmholtz(3, 12, mach=0.3, rmn=P.RMN_MLAU),
+             P.smooth_wave(2, 24, rmn=P.RMN_ROE), P.kelvin_helmholtz(2, 32, mach=0.3, rmn=P.RMN_LHLLD)]
+    want = [restatement.run(p, 3, mode=R.MODE_RUN)["state"] for p in probs]
+    got = [None] * len(probs)
+    errs = []
+
+    def work(q):
+        try:
+            p = probs[q]
+            with L.Context.from_problem(p) as ctx:
+                ctx.upload(p.state)
+                ctx.run(max_steps=3, flg=1, stop_rule=0, cfl=p.cfl)
+                got[q] = ctx.download(p.state.shape)
+        except Exception as e:  # reported below, on the test's thread
+            errs.append(e)
+
+    threads = [threading.Thread(target=work, args=(q,)) for q in range(len(probs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errs, errs
+    for q in range(len(probs)):
+        assert_bitwise(got[q], want[q], probs[q].name)
+
+
 def test_cfl_reduction_matches(restatement):
     p = P.kelvin_helmholtz(3, 12, mach=0.4)
     import ctypes
