@@ -409,6 +409,11 @@ qas_status qas_dd_kernel_launches(const qas_dd *dd, long long *kernels, long lon
  * ------------------------------------------------------------------------------------ */
 qas_status qas_adjoint_forward(qas_ctx *ctx, int nsteps, int ckpt_every, const double *dts, double eta0);
 qas_status qas_adjoint_backward(qas_ctx *ctx, const double *dldu_final, double *dldu0, double *dldeta0);
+/* Both in one call, for a loss whose gradient with respect to the final state is known before
+ * the run (a loss linear in the final state, such as a weighted sum of its fields):
+ * qas_adjoint_forward, then qas_adjoint_backward with dldu_final; same results, same status. */
+qas_status qas_adjoint_run(qas_ctx *ctx, int nsteps, int ckpt_every, const double *dts, double eta0,
+                           const double *dldu_final, double *dldu0, double *dldeta0);
 
 /* ------------------------------------------------------------------------------------
  * Allocation-free max |div B| (no counterpart in the reference, whose caller owns host

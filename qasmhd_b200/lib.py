@@ -38,7 +38,7 @@ EXPORTS = (
     "qas_kernel_launches", "qas_bc_map", "qas_profile_run", "qas_set_option", "qas_set_tile",
     "qas_get_tile", "qas_autotune", "qas_batch_create", "qas_batch_destroy", "qas_batch_cells",
     "qas_batch_upload", "qas_batch_download", "qas_batch_run", "qas_batch_set_tile", "qas_batch_autotune",
-    "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward",
+    "qas_batch_stream", "qas_batch_kernel_launches", "qas_fp64_peak", "qas_adjoint_forward", "qas_adjoint_run",
     "qas_adjoint_backward", "qas_max_divb_noalloc", "qas_dout", "qas_dout_wait", "qas_bkup_save",
     "qas_bkup_load", "qas_dd_plan", "qas_dd_create", "qas_dd_destroy", "qas_dd_upload_block",
     "qas_dd_download_block", "qas_dd_run", "qas_dd_parts", "qas_dd_kernel_launches", "qas_set_gravity",
@@ -165,6 +165,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.qas_fp64_peak.argtypes = [dp]
     lib.qas_adjoint_forward.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double]
     lib.qas_adjoint_backward.argtypes = [vp, dp, dp, dp]
+    lib.qas_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp, dp, dp]
     lib.qas_dout.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                              ctypes.POINTER(dp)]
     lib.qas_dout_wait.argtypes = [vp]
@@ -464,6 +465,18 @@ class Context:
         out = np.empty((8, self.nd), dtype=np.float64)
         eb = ctypes.c_double()
         _check(self.lib.qas_adjoint_backward(self.h, _dptr(g), _dptr(out), ctypes.byref(eb)), "qas_adjoint_backward")
+        return out, eb.value
+
+    def adjoint_run(self, dts: Sequence[float], dldu: np.ndarray, eta0: float = 0.0, ckpt_every: int = 20):
+        """adjoint_forward then adjoint_backward in one call (qas_adjoint_run), for a known
+        dL/d(final state): returns (dL/d(initial state) as (8, nd), dL/deta0)."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        g = np.ascontiguousarray(dldu, dtype=np.float64).reshape(8, -1)
+        assert g.shape[1] == self.nd
+        out = np.empty((8, self.nd), dtype=np.float64)
+        eb = ctypes.c_double()
+        _check(self.lib.qas_adjoint_run(self.h, int(d.size), int(ckpt_every), _dptr(d), float(eta0), _dptr(g),
+                                        _dptr(out), ctypes.byref(eb)), "qas_adjoint_run")
         return out, eb.value
 
     def max_divb(self) -> float:

@@ -128,6 +128,26 @@ def test_refused_configurations():
             ctx.adjoint_forward([1e-3, -1.0], 0.0, 1)
 
 
+def test_adjoint_run_one_call_equals_the_pair():
+    """qas_adjoint_run (forward and backward in one call) gives the bits of qas_adjoint_forward
+    followed by qas_adjoint_backward, and leaves the same final state."""
+    prob = smooth_wave(2, 24, rmn=RMN_ROE)
+    eta = 1e-3
+    u0 = prob.state.reshape(8, -1).copy()
+    w = np.random.default_rng(4).standard_normal(u0.shape)
+    with L.Context.from_problem(prob) as ctx:
+        dts = cfl_dts(ctx, u0, 4, prob.cfl, eta)
+        ctx.upload(u0)
+        ctx.adjoint_forward(dts, eta, 2)
+        fin_a = ctx.download()
+        g_a, e_a = ctx.adjoint_backward(w)
+        ctx.upload(u0)
+        g_b, e_b = ctx.adjoint_run(dts, w, eta, 2)
+        fin_b = ctx.download()
+    assert np.array_equal(fin_a, fin_b)
+    assert np.array_equal(g_a, g_b) and e_a == e_b
+
+
 def test_autograd_function_kh_inversion_small():
     P = KHInverse(n=32, nsteps=20, ckpt_every=6)
     try:
