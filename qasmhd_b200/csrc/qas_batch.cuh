@@ -77,8 +77,29 @@ __device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, 
 
 #define QAS_BATCH_CELL_OK (ti < v.g.nx && tj < v.g.ny && tk < v.g.nz)
 
+// resident-block caps of the light batched kernels (0: the single-grid kernels' 16).  The block
+// loop keeps the instance View and map entry live, so at the single-grid cap (32 registers) both
+// spill (96-180 B); at 8 blocks (64 registers) neither does.  Measured on the 512-member C4
+// ensemble, same box back to back: 580-582 (16), 573-576 (12), 592-593 (8) Mcell-updates/s.
+#ifndef QAS_BATCH_PRIM_MINB
+#define QAS_BATCH_PRIM_MINB 8
+#endif
+#ifndef QAS_BATCH_UPDATE_MINB
+#define QAS_BATCH_UPDATE_MINB 8
+#endif
+#if QAS_BATCH_PRIM_MINB > 0
+#define QAS_BATCH_PRIM_BOUNDS __launch_bounds__(128, QAS_BATCH_PRIM_MINB)
+#else
+#define QAS_BATCH_PRIM_BOUNDS QAS_PRIM_BOUNDS
+#endif
+#if QAS_BATCH_UPDATE_MINB > 0
+#define QAS_BATCH_UPDATE_BOUNDS __launch_bounds__(128, QAS_BATCH_UPDATE_MINB)
+#else
+#define QAS_BATCH_UPDATE_BOUNDS QAS_UPDATE_BOUNDS
+#endif
+
 template <int ODR>
-__global__ void QAS_PRIM_BOUNDS kb_prim(const View *__restrict__ views, BMap map)
+__global__ void QAS_BATCH_PRIM_BOUNDS kb_prim(const View *__restrict__ views, BMap map)
 {
   QAS_BATCH_BLOCKS(map)
   if (QAS_BATCH_CELL_OK) prim_body<ODR>(v, ti, tj, tk);
@@ -140,7 +161,7 @@ __global__ void kb_emf(const View *__restrict__ views, BMap map)
 }
 
 template <int ODR>
-__global__ void QAS_UPDATE_BOUNDS kb_update(const View *__restrict__ views, BMap map, double c0, double c1)
+__global__ void QAS_BATCH_UPDATE_BOUNDS kb_update(const View *__restrict__ views, BMap map, double c0, double c1)
 {
   QAS_BATCH_BLOCKS(map)
   int i, j, k;
