@@ -80,12 +80,14 @@ __device__ __forceinline__ void batch_thread(int4 gd, int lb, int &ti, int &tj, 
 // resident-block caps of the light batched kernels (0: the single-grid kernels' 16).  The block
 // loop keeps the instance View and map entry live, so at the single-grid cap (32 registers) both
 // spill (96-180 B); at 8 blocks (64 registers) neither does.  Measured on the 512-member C4
-// ensemble, same box back to back: 580-582 (16), 573-576 (12), 592-593 (8) Mcell-updates/s.
+// ensemble, same box back to back: both at 16 / 12 / 8 blocks 580-582 / 573-576 / 592-593
+// Mcell-updates/s; with the primitives at 8, the update at 16 / 12 / 8 594-598 / 583-586 /
+// 594-597 -- the gain is the primitives', so the update keeps the single-grid cap.
 #ifndef QAS_BATCH_PRIM_MINB
 #define QAS_BATCH_PRIM_MINB 8
 #endif
 #ifndef QAS_BATCH_UPDATE_MINB
-#define QAS_BATCH_UPDATE_MINB 8
+#define QAS_BATCH_UPDATE_MINB 0
 #endif
 #if QAS_BATCH_PRIM_MINB > 0
 #define QAS_BATCH_PRIM_BOUNDS __launch_bounds__(128, QAS_BATCH_PRIM_MINB)
