@@ -796,10 +796,13 @@ __device__ __forceinline__ double d4(const double *p, long long c, long long s)
   return dfc<ODR>(p[c - s], p[c], p[c + s], p[c + 2 * s]);
 }
 
-// update cell (i,j,k), i in [GH, nx-GH] etc.: the extra face of the staggered fields included
+// update cell (i,j,k), i in [GH, nx-GH] etc.: the extra face of the staggered fields included.
+// The stage input is read from uin (default: the state v.u itself, updated in place)
 template <int ODR>
-__device__ __forceinline__ void update_body(const View &v, int i, int j, int k, double c0, double c1)
+__device__ __forceinline__ void update_body(const View &v, int i, int j, int k, double c0, double c1,
+                                            double *const *uin = nullptr)
 {
+  double *const *const ui = uin ? uin : v.u;
   const Geo &g = v.g;
   const long long c = cidx(g, i, j, k);
   const double dtdx = v.ctl->dtd[0], dtdy = v.ctl->dtd[1], dtdz = v.ctl->dtd[2];
@@ -832,7 +835,7 @@ __device__ __forceinline__ void update_body(const View &v, int i, int j, int k, 
           du = (-dtdx * du0 - dtdy * du1 - dtdz * du2);
         }
       }
-      nv[m] = rk_combine(v.u[m][c], v.u0[m][c], du, c0, c1);
+      nv[m] = rk_combine(ui[m][c], v.u0[m][c], du, c0, c1);
       wr[m] = true;
     }
     if (v.phi) {
@@ -847,31 +850,31 @@ __device__ __forceinline__ void update_body(const View &v, int i, int j, int k, 
   if (g.dim == 2) {
     if (cj) {  // bx on i in [GH, nx-GH]
       const double du = d4<ODR>(v.ez, c, sy);
-      nv[4] = rk_combine(v.u[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
+      nv[4] = rk_combine(ui[4][c], v.u0[4][c], -(+dtdy) * du, c0, c1);
       wr[4] = true;
     }
     if (ci && j <= g.ny - GH) {  // by on j in [GH, ny-GH]
       const double du = d4<ODR>(v.ez, c, 1);
-      nv[5] = rk_combine(v.u[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
+      nv[5] = rk_combine(ui[5][c], v.u0[5][c], -(-dtdx) * du, c0, c1);
       wr[5] = true;
     }
   } else if (g.dim == 3) {
     if (ck && cj) {
       const double du0 = +d4<ODR>(v.ez, c, sy);
       const double du1 = -d4<ODR>(v.ey, c, sz);
-      nv[4] = rk_combine(v.u[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
+      nv[4] = rk_combine(ui[4][c], v.u0[4][c], -dtdy * du0 - dtdz * du1, c0, c1);
       wr[4] = true;
     }
     if (ck && ci) {
       const double du0 = +d4<ODR>(v.ex, c, sz);
       const double du1 = -d4<ODR>(v.ez, c, 1);
-      nv[5] = rk_combine(v.u[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
+      nv[5] = rk_combine(ui[5][c], v.u0[5][c], -dtdz * du0 - dtdx * du1, c0, c1);
       wr[5] = true;
     }
     if (cj && ci) {
       const double du0 = +d4<ODR>(v.ey, c, 1);
       const double du1 = -d4<ODR>(v.ex, c, sy);
-      nv[6] = rk_combine(v.u[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
+      nv[6] = rk_combine(ui[6][c], v.u0[6][c], -dtdx * du0 - dtdy * du1, c0, c1);
       wr[6] = true;
     }
   }

@@ -52,9 +52,10 @@ __device__ __forceinline__ bool win_cell(const Geo &g, const Rows2 &r, int &i, i
   return h >= 0 && i < g.nx && j < g.ny && k < g.nz;
 }
 
-// the primitives on planes pr and the copy of the eight state arrays v.u -> dst on planes cp, one
-// launch over rows r (their union); the copy ignores the stop flag (a finished run carries its
-// state through)
+// the primitives on planes pr, one launch over rows r (pr and cp together); on a finished run
+// (stop flag set) instead the copy of the eight state arrays v.u -> dst on planes cp, so that the
+// state passes through unchanged (otherwise the update writes every interior cell of dst from
+// v.u and the ghost fill the rest)
 template <int ODR>
 __global__ void QAS_PRIM_BOUNDS kw_prim_copy(View v, Rows2 r, Rows2 pr, Rows2 cp, StatePtrs dst)
 {
@@ -62,7 +63,7 @@ __global__ void QAS_PRIM_BOUNDS kw_prim_copy(View v, Rows2 r, Rows2 pr, Rows2 cp
   int i, j, k;
   if (!win_cell(v.g, r, i, j, k)) return;
   const int h = v.g.dim == 3 ? k : j;
-  if (rows2_has(cp, h)) {
+  if (v.ctl->done && rows2_has(cp, h)) {
     const long long c = cidx(v.g, i, j, k);
 #pragma unroll
     for (int m = 0; m < 8; m++) dst.p[m][c] = v.u[m][c];
@@ -185,7 +186,7 @@ __global__ void QAS_EMF_BOUNDS kw_emf(View v, Rows2 r)
 // the update cells of k_update (i in [GH, nx-GH], likewise j in 3D) on planes [lo, hi), which
 // lie in [GH, n-GH] (the last face plane of the staggered field included)
 template <int ODR>
-__global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows2 r, double c0, double c1)
+__global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows2 r, double c0, double c1, StatePtrs src)
 {
   QAS_PDL_WAIT();
   if (v.ctl->done) return;
@@ -204,7 +205,7 @@ __global__ void QAS_UPDATE_BOUNDS kw_update(View v, Rows2 r, double c0, double c
     if (tk > 0 || j < 0) return;
   }
   if (i > g.nx - GH) return;
-  update_body<ODR>(v, i, j, k, c0, c1);
+  update_body<ODR>(v, i, j, k, c0, c1, src.p);  // U_r of the cell from U_{r-1} (src) and ut
 }
 
 // ghost fill of the cells of planes [lo, hi) that are ghosts along an in-plane axis (x in 2D;
