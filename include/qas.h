@@ -422,8 +422,7 @@ qas_status qas_adjoint_run(qas_ctx *ctx, int nsteps, int ckpt_every, const doubl
  * It serves callers whose device memory is all handed to an arena or caching allocator
  * under a fixed budget (a framework's memory pool), where a library cudaMalloc would fail
  * or eat into that budget.  It is a synchronous host query: it ends with a device-to-host
- * copy of the result and synchronises `stream`, so it must not be called while that
- * stream is being captured into a CUDA graph.
+ * copy of the result and synchronises `stream`.
  * d_state: 8 fields of the reference's ghost-padded layout, field m at d_state +
  * m*field_stride (field_stride >= nd); stream: a cudaStream_t (NULL = default stream).
  * Scratch is a static 512 KiB device array (every device that loads the library holds it
